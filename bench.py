@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Throughput of the fused Henon-map tracking path on B200.
+
+Workload (the modulated dynamic-aperture scan): a 1024x1024 grid of initial
+conditions x0, y0 in [0, 0.6], px0 = py0 = 0, tunes (0.168, 0.201), SPS
+modulation with epsilon in {1, 16, 64} and mu in {0, 0.2}, barrier 10,
+10^5 turns.  One step = the six (epsilon, mu) scans, each a full tracking
+pass of the 2^20 particles.  Synthetic, deterministic inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value      : nominal particle-turns/s over the whole job (particles x turns,
+             lost particles counted as tracked -- the reference's own
+             convention), inputs resident in HBM, CUDA events on the launch
+             stream, max over ranks.
+e2e        : the same metric through the public API with host buffers:
+             pinned host arrays -> particles -> track -> steps read back.
+roofline   : executed FP64 flops (survivor-turns x 26 or 42) / summed device
+             time of the tracking kernels, against the FP64 FMA-chain peak
+             measured in the same process.
+cpu_baseline: the reference's own CPU path (built from its sources by
+             oracle/build_ref.sh) on a strided subsample of the grid, all
+             host cores; reported, not a target.
+Multi-GPU (torchrun): each rank scans its own 2^20-particle interleaved
+slice of a 1024 x (1024 N) grid; no collective in the data path ("weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "FP64 particle-turns/s (% FP64 peak); batched and adjoint vs plain, same GPU"
+UNIT = "particle-turns/s"
+TUNES = (0.168, 0.201)
+EPSILONS = (1.0, 16.0, 64.0)
+MUS = (0.0, 0.2)
+BARRIER = 10.0
+FLOPS_PER_TURN = {False: 26.0, True: 42.0}  # mu == 0 / mu != 0 (algorithmic)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--turns", type=int, default=100_000)
+    ap.add_argument("--side", type=int, default=1024)
+    ap.add_argument("--arith", choices=["exact", "fast"], default="exact")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args, n_gpus):
+    return {"workload": "modulated DA scan: 1024x1024 grid x0,y0 in [0,0.6], px0=py0=0, "
+                        "SPS eps in {1,16,64} x mu in {0,0.2}, 1e5 turns, barrier 10",
+            "particles_per_gpu": args.side * args.side, "turns": args.turns,
+            "epsilon": list(EPSILONS), "mu": list(MUS), "tunes": list(TUNES),
+            "arith": args.arith, "parallelism": f"particle shards x{n_gpus}",
+            "l2": "flushed between steps (256 MiB write); state < L2, compute-bound"}
+
+
+def grid_slice(side: int, rank: int, world: int):
+    """Rank's interleaved slice of a side x (side*world) grid on [0, 0.6]^2."""
+    xs = np.linspace(0.0, 0.6, side * world)[rank::world]
+    ys = np.linspace(0.0, 0.6, side)
+    xx, yy = np.meshgrid(xs, ys)
+    x = np.ascontiguousarray(xx.ravel())
+    y = np.ascontiguousarray(yy.ravel())
+    return x, np.zeros_like(x), y, np.zeros_like(y)
+
+
+# ---- clocks --------------------------------------------------------------------
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self):
+        mhz, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                mhz.append(float(parts[0]))
+                maxs.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not mhz:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxs),
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ---- CPU baseline (the reference's own CPU path) -----------------------------------
+
+def reference_cpu_sample(turns: int, side: int, target_s: float = 20.0):
+    """Runs the reference CPU tracker on a strided subsample of the grid for
+    all six (eps, mu) scans; grows the sample until it takes ~target_s."""
+    from oracle import oracle as O
+
+    R = O.reference_module("default") or O.reference_module("fmad_off")
+    kind = "reference"
+    if R is None:
+        kind = "port"
+    x, px, y, py = grid_slice(side, 0, 1)
+    stride = 32
+    while True:
+        sel = np.zeros((side, side), bool)
+        sel[::stride, ::stride] = True
+        sel = sel.ravel()
+        sx, spx, sy, spy = (np.ascontiguousarray(a[sel]) for a in (x, px, y, py))
+        n = sx.size
+        t0 = time.perf_counter()
+        for eps in EPSILONS:
+            if kind == "reference":
+                tr = R.henon_tracker(turns, TUNES[0], TUNES[1], "sps", float("nan"), eps, 0)
+            else:
+                tabs = O.tables(turns, TUNES[0], TUNES[1], "sps", epsilon=eps)
+            for mu in MUS:
+                if kind == "reference":
+                    p = R.particles_4d(sx, spx, sy, spy)
+                    tr.track(p, turns, mu, BARRIER)
+                else:
+                    O.track(sx, spx, sy, spy, np.zeros(n, np.uint32), tabs, turns, mu, BARRIER)
+        dt = time.perf_counter() - t0
+        if dt >= target_s / 4 or stride <= 4:
+            break
+        stride //= 2
+    nominal = n * turns * len(EPSILONS) * len(MUS)
+    cores = os.cpu_count() if kind == "reference" else O.max_threads()
+    return {"value": nominal / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"every {stride}th grid point per axis ({n} particles) x {turns} turns x "
+                      f"6 (eps, mu) scans = {nominal:.3g} nominal particle-turns in {dt:.2f} s "
+                      f"(table setup included)"}
+
+
+# ---- reference arm ---------------------------------------------------------------
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        reference_cpu_sample(args.turns, args.side, target_s=4.0)
+    vals, times = [], []
+    res = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = reference_cpu_sample(args.turns, args.side, target_s=12.0)
+        times.append(time.perf_counter() - t0)
+        vals.append(res["value"])
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, 1), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"],
+                             "kind": res["kind"], "sample": res["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm -----------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from henon_map_cpp_b200 import _capi as C  # fails loudly if the library is missing
+
+    arith = C.ARITH_FAST if args.arith == "fast" else C.ARITH_EXACT
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    peak_tflops, _ = C.fp64_peak(0.3)
+
+    trackers = {eps: C.Tracker(args.turns, TUNES[0], TUNES[1], "sps", float("nan"), eps, 0)
+                for eps in EPSILONS}
+    x0, px0, y0, py0 = grid_slice(args.side, rank, world)
+    n = x0.size
+    dev0 = [torch.from_numpy(a).cuda() for a in (x0, px0, y0, py0)]
+    work = [torch.empty_like(d) for d in dev0]
+    steps = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ws = torch.empty(C.load().hm_track_workspace_bytes(n), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def one_step(mode):
+        executed = 0.0
+        flops = 0.0
+        for eps in EPSILONS:
+            tab = trackers[eps].device_tables()
+            for mu in MUS:
+                for w, d in zip(work, dev0):
+                    w.copy_(d)
+                steps.zero_()
+                C.call("hm_track_device", *[w.data_ptr() for w in work], steps.data_ptr(), n,
+                       tab, args.turns, 0, args.turns, mu, BARRIER, 0, mode, ws.data_ptr(), sptr)
+                s = float(steps.sum(dtype=torch.int64).item())
+                executed += s
+                flops += s * FLOPS_PER_TURN[mu != 0.0]
+        return executed, flops
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(mode, n_steps, n_warm):
+        for _ in range(n_warm):
+            one_step(mode)
+        barrier()
+        C.set_profiling(True)
+        total_ms, executed, flops = 0.0, 0.0, 0.0
+        for _ in range(n_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e, f = one_step(mode)
+            b.record(stream)
+            b.synchronize()
+            total_ms += a.elapsed_time(b)
+            executed += e
+            flops += f
+        kernel_ms, launches = C.get_profile()
+        C.set_profiling(False)
+        barrier()
+        return total_ms, executed, flops, kernel_ms, launches
+
+    with ClockSampler(local) as clocks:
+        total_ms, executed, flops, kernel_ms, launches = timed(arith, args.steps, args.warmup)
+    clock_summary = clocks.summary()
+
+    # Whole-job numbers: max time over ranks, sum of work.
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        w = torch.tensor([executed, flops], dtype=torch.float64, device="cuda")
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        executed, flops = (float(v) for v in w.tolist())
+    nominal = float(n) * args.turns * len(EPSILONS) * len(MUS) * args.steps * world
+    value = nominal / (total_ms * 1e-3)
+
+    # Roofline of the tracking kernel on this rank (per-launch average).
+    local_flops = flops / world if dist is not None else flops
+    achieved_tf = local_flops / (kernel_ms * 1e-3) / 1e12 if kernel_ms > 0 else 0.0
+
+    # The other arithmetic, for reference (not the headline).
+    other = C.ARITH_EXACT if arith == C.ARITH_FAST else C.ARITH_FAST
+    o_ms, o_exec, o_flops, o_kms, _ = timed(other, 1, 1)
+    o_tf = o_flops / (o_kms * 1e-3) / 1e12 if o_kms > 0 else 0.0
+    if dist is not None:
+        t = torch.tensor([o_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        o_ms = float(t.item())
+    o_value = float(n) * args.turns * 6 * world / (o_ms * 1e-3)
+
+    # End to end through the public API with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        pinned = [torch.from_numpy(a).pin_memory().numpy() for a in (x0, px0, y0, py0)]
+        out_steps = torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+
+        def e2e_step():
+            for eps in EPSILONS:
+                for mu in MUS:
+                    p = C.Particles(*pinned)
+                    p_tr = trackers[eps]
+                    p_tr.arith = arith
+                    p_tr.track(p, args.turns, mu, BARRIER)
+                    C.call("hm_particles_get", p.h, C.FIELD_STEPS,
+                           out_steps.ctypes.data_as(C.c_void_p))
+                    del p
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": float(n) * args.turns * 6 * world / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": 6 * 4 * 8 * n, "d2h_bytes_per_step": 6 * 4 * n,
+               "path": "hm_particles_create (pinned host) -> hm_track -> hm_particles_get(steps)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = reference_cpu_sample(args.turns, args.side)
+
+    if rank == 0:
+        peak_unit = "TFLOP/s"
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, world),
+            "executed_particle_turns_per_s": executed / (total_ms * 1e-3),
+            "survivor_fraction": executed / nominal,
+            "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tflops,
+                         "unit": peak_unit, "frac": achieved_tf / peak_tflops if peak_tflops else None,
+                         "traffic": None,
+                         "peak_source": "FP64 FMA-chain microbenchmark in this process "
+                                        "(hm_fp64_peak; FMA = 2 flops)",
+                         "kernel": "track_chunk_kernel", "kernel_ms": kernel_ms,
+                         "launches": launches},
+            "other_arith": {"arith": "fast" if other == C.ARITH_FAST else "exact",
+                            "value": o_value, "achieved_tflops": o_tf,
+                            "frac": o_tf / peak_tflops if peak_tflops else None},
+            "gpu_launches": launches,
+            "clocks": clock_summary,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

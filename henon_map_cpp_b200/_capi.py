@@ -1,0 +1,287 @@
+"""ctypes binding of the C ABI in include/henon_b200.h (libhenon_b200.so).
+
+This is the thinnest host layer: every call maps 1:1 to an `hm_*` entry
+point and a non-OK status raises the matching Python exception with the
+library's message.  The library is loaded from this package's directory and
+nowhere else; a missing library raises at import time of the caller.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_int, c_size_t, c_uint32, c_uint64, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libhenon_b200.so"
+
+HM_OK = 0
+HM_ERR_INVALID_ARG = 1
+HM_ERR_BUDGET = 2
+HM_ERR_CUDA = 3
+HM_ERR_TIMEOUT = 4
+HM_ERR_CANCELLED = 5
+HM_ERR_OOM = 6
+HM_ERR_UNKNOWN_MODULATION = 7
+HM_ERR_NOT_SUPPORTED = 8
+HM_ERR_NO_DEVICE = 9
+
+ARITH_EXACT = 0
+ARITH_FAST = 1
+
+FIELD_X, FIELD_PX, FIELD_Y, FIELD_PY, FIELD_STEPS, FIELD_VALID, FIELD_GHOST, FIELD_IDX, \
+    FIELD_IDX_BASE = range(9)
+FIELD_DTYPE = {FIELD_X: np.float64, FIELD_PX: np.float64, FIELD_Y: np.float64,
+               FIELD_PY: np.float64, FIELD_STEPS: np.uint32, FIELD_VALID: np.uint8,
+               FIELD_GHOST: np.uint8, FIELD_IDX: np.uint64, FIELD_IDX_BASE: np.uint64}
+
+OBS_RADIUS, OBS_ACTION, OBS_ACTION_X, OBS_ACTION_Y, OBS_ANGLE_X, OBS_ANGLE_Y = range(6)
+
+
+class HMError(RuntimeError):
+    """A non-OK hm_status; `.status` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class HMCancelled(HMError):
+    """The cancel callback stopped an operation (state left consistent)."""
+
+
+_PD = POINTER(c_double)
+_PU32 = POINTER(c_uint32)
+
+# name -> (restype, argtypes); restype None means hm_status (checked).
+_SIGNATURES = {
+    "hm_last_error": (c_char_p, []),
+    "hm_version": (c_int, []),
+    "hm_device_count": (c_int, []),
+    "hm_set_cancel_callback": (None, [c_void_p, c_void_p]),
+    "hm_set_track_config": (None, [c_int, c_int, c_uint32, c_uint32]),
+    "hm_get_track_config": (None, [POINTER(c_int), POINTER(c_int), _PU32, _PU32]),
+    "hm_modulation": (None, [c_char_p, c_uint32, c_double, c_double, c_double, c_double,
+                             c_uint32, _PD, _PD]),
+    "hm_sps_modulation": (None, [c_double, c_double, ctypes.c_int32, ctypes.c_int32, _PD]),
+    "hm_basic_modulation": (None, [c_double, c_double, c_double, ctypes.c_int32,
+                                   ctypes.c_int32, _PD]),
+    "hm_birkhoff_weights": (None, [c_uint32, _PD]),
+    "hm_tracker_create": (None, [c_uint32, c_double, c_double, c_char_p, c_double, c_double,
+                                 c_uint32, POINTER(c_void_p)]),
+    "hm_tracker_compute_a_modulation": (None, [c_void_p, c_uint32, c_double, c_double, c_char_p,
+                                               c_double, c_double, c_uint32]),
+    "hm_tracker_destroy": (None, [c_void_p]),
+    "hm_tracker_allowed_steps": (None, [c_void_p, POINTER(c_uint64)]),
+    "hm_tracker_get_tables": (None, [c_void_p, _PD, _PD, _PD, _PD]),
+    "hm_tracker_device_tables": (None, [c_void_p, POINTER(c_void_p)]),
+    "hm_tracker_set_arith": (None, [c_void_p, c_int]),
+    "hm_tracker_get_arith": (None, [c_void_p, POINTER(c_int)]),
+    "hm_particles_create": (None, [_PD, _PD, _PD, _PD, c_size_t, POINTER(c_void_p)]),
+    "hm_particles_destroy": (None, [c_void_p]),
+    "hm_particles_reset": (None, [c_void_p]),
+    "hm_particles_size": (None, [c_void_p, POINTER(c_size_t), POINTER(c_size_t),
+                                 POINTER(c_size_t)]),
+    "hm_particles_global_steps": (None, [c_void_p, _PU32]),
+    "hm_particles_get": (None, [c_void_p, c_int, c_void_p]),
+    "hm_particles_device_ptr": (None, [c_void_p, c_int, POINTER(c_void_p)]),
+    "hm_particles_observable": (None, [c_void_p, c_int, _PD]),
+    "hm_track": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, c_double, c_int]),
+    "hm_track_workspace_bytes": (c_size_t, [c_size_t]),
+    "hm_track_device": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+                               c_void_p, c_uint64, c_uint32, c_uint32, c_double, c_double, c_int,
+                               c_int, c_void_p, c_void_p]),
+    "hm_fp64_peak": (None, [c_double, _PD, _PD]),
+    "hm_set_profiling": (None, [c_int]),
+    "hm_get_profile": (None, [_PD, POINTER(c_uint64)]),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads libhenon_b200.so from the package directory (raises if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m henon_map_cpp_b200.build`")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGNATURES.items():
+        if not hasattr(lib, name):
+            continue  # declared later in the header than this binding knows
+        fn = getattr(lib, name)
+        fn.restype = c_int if res is None else res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().hm_last_error().decode()
+
+
+_EXC = {HM_ERR_INVALID_ARG: ValueError, HM_ERR_NOT_SUPPORTED: NotImplementedError,
+        HM_ERR_OOM: MemoryError}
+
+
+def check(status: int) -> None:
+    if status == HM_OK:
+        return
+    msg = last_error()
+    if status == HM_ERR_CANCELLED:
+        raise HMCancelled(status, msg)
+    base = _EXC.get(status)
+    if base is None:
+        raise HMError(status, msg)
+    err = type(f"HM{base.__name__}", (HMError, base), {})(status, msg)
+    raise err
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_PD)
+
+
+def f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ---- handle wrappers (ownership: the wrapper destroys its handle) -----------------
+
+class Tracker:
+    """hm_tracker: modulation tables on the device (henon_tracker_gpu)."""
+
+    def __init__(self, n_turns: int, omega_x: float, omega_y: float, kind: str = "sps",
+                 omega_0: float = float("nan"), epsilon: float = 0.0, offset: int = 0):
+        self.h = c_void_p()
+        call("hm_tracker_create", int(n_turns), float(omega_x), float(omega_y), kind.encode(),
+             float(omega_0), float(epsilon), int(offset), ctypes.byref(self.h))
+
+    def compute_a_modulation(self, n_turns, omega_x, omega_y, kind="sps",
+                             omega_0=float("nan"), epsilon=0.0, offset=0):
+        call("hm_tracker_compute_a_modulation", self.h, int(n_turns), float(omega_x),
+             float(omega_y), kind.encode(), float(omega_0), float(epsilon), int(offset))
+
+    @property
+    def allowed_steps(self) -> int:
+        v = c_uint64()
+        call("hm_tracker_allowed_steps", self.h, ctypes.byref(v))
+        return int(v.value)
+
+    def tables(self):
+        n = self.allowed_steps
+        out = [np.empty(n) for _ in range(4)]
+        call("hm_tracker_get_tables", self.h, *map(dptr, out))
+        return tuple(out)
+
+    def device_tables(self) -> int:
+        v = c_void_p()
+        call("hm_tracker_device_tables", self.h, ctypes.byref(v))
+        return int(v.value or 0)
+
+    @property
+    def arith(self) -> int:
+        v = c_int()
+        call("hm_tracker_get_arith", self.h, ctypes.byref(v))
+        return int(v.value)
+
+    @arith.setter
+    def arith(self, mode: int) -> None:
+        call("hm_tracker_set_arith", self.h, int(mode))
+
+    def track(self, particles: "Particles", n_turns: int, mu: float, barrier: float = 100.0,
+              kick_module: float = float("nan"), inverse: bool = False) -> None:
+        call("hm_track", self.h, particles.h, int(n_turns), float(mu), float(barrier),
+             float(kick_module), int(bool(inverse)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib is not None:
+            _lib.hm_tracker_destroy(self.h)
+            self.h = c_void_p()
+
+
+class Particles:
+    """hm_particles: particle ensemble on the device (particles_4d_gpu)."""
+
+    def __init__(self, x, px, y, py):
+        x, px, y, py = (f64(a) for a in (x, px, y, py))
+        if not (x.shape == px.shape == y.shape == py.shape) or x.ndim != 1:
+            raise ValueError("x, px, y, py must be 1D arrays of the same shape")
+        self.h = c_void_p()
+        call("hm_particles_create", dptr(x), dptr(px), dptr(y), dptr(py), x.size,
+             ctypes.byref(self.h))
+
+    def size(self):
+        a, b, c = c_size_t(), c_size_t(), c_size_t()
+        call("hm_particles_size", self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return int(a.value), int(b.value), int(c.value)
+
+    @property
+    def n_total(self) -> int:
+        return self.size()[0]
+
+    @property
+    def global_steps(self) -> int:
+        v = c_uint32()
+        call("hm_particles_global_steps", self.h, ctypes.byref(v))
+        return int(v.value)
+
+    def get(self, field: int) -> np.ndarray:
+        out = np.empty(self.n_total, dtype=FIELD_DTYPE[field])
+        call("hm_particles_get", self.h, field, out.ctypes.data_as(c_void_p))
+        return out
+
+    def device_ptr(self, field: int) -> int:
+        v = c_void_p()
+        call("hm_particles_device_ptr", self.h, field, ctypes.byref(v))
+        return int(v.value or 0)
+
+    def observable(self, kind: int) -> np.ndarray:
+        out = np.empty(self.n_total)
+        call("hm_particles_observable", self.h, kind, dptr(out))
+        return out
+
+    def state(self):
+        return (self.get(FIELD_X), self.get(FIELD_PX), self.get(FIELD_Y), self.get(FIELD_PY),
+                self.get(FIELD_STEPS))
+
+    def reset(self) -> None:
+        call("hm_particles_reset", self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib is not None:
+            _lib.hm_particles_destroy(self.h)
+            self.h = c_void_p()
+
+
+def set_track_config(threads: int, per_thread: int, chunk0: int, chunk_max: int) -> None:
+    call("hm_set_track_config", int(threads), int(per_thread), int(chunk0), int(chunk_max))
+
+
+def get_track_config():
+    a, b, c, d = c_int(), c_int(), c_uint32(), c_uint32()
+    call("hm_get_track_config", ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+         ctypes.byref(d))
+    return int(a.value), int(b.value), int(c.value), int(d.value)
+
+
+def set_profiling(on: bool) -> None:
+    call("hm_set_profiling", int(bool(on)))
+
+
+def get_profile():
+    """(summed kernel ms, launches) of the tracking kernels since profiling began."""
+    ms, n = c_double(), c_uint64()
+    call("hm_get_profile", ctypes.byref(ms), ctypes.byref(n))
+    return float(ms.value), int(n.value)
+
+
+def fp64_peak(seconds: float = 0.2):
+    """(TFLOP/s, ms) of the FP64 FMA-chain microbenchmark on the current device."""
+    tf, ms = c_double(), c_double()
+    call("hm_fp64_peak", float(seconds), ctypes.byref(tf), ctypes.byref(ms))
+    return float(tf.value), float(ms.value)

@@ -1,0 +1,772 @@
+// C ABI of libhenon_b200.so: handles, validation, error reporting and the
+// host driver of the chunked tracking launches.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "hm_internal.h"
+
+// ---- handles ------------------------------------------------------------------
+
+// Particle ensemble on the device (particles_4d_gpu, src/henon.h:119-193).
+struct hm_particles {
+    size_t n_total = 0;      // base particles + ghosts
+    size_t n_particles = 0;  // base particles
+    size_t n_ghosts = 0;     // ghosts per base particle
+    uint32_t global_steps = 0;
+    // steps value shared by every live (non-NaN) particle: all particles
+    // start at 0, survivors advance together and lost ones are frozen as NaN,
+    // so the table index of a whole track() call is uniform.
+    uint32_t live_step = 0;
+    // Host copies of what the reference keeps on the host side.
+    std::vector<double> x0, px0, y0, py0;
+    std::vector<uint8_t> valid, ghost;
+    std::vector<uint64_t> idx, idx_base;
+    hm::DeviceBuffer x, px, y, py, steps, dvalid, dghost, didx, didx_base;
+    hm::DeviceBuffer work;  // survivor lists of the chunked tracker
+    uint64_t rng_state = 0x9e3779b97f4a7c15ULL;
+};
+
+// Modulation tables on the device (henon_tracker_gpu, src/henon.h:212-228).
+struct hm_tracker {
+    uint64_t allowed_steps = 0;
+    std::vector<double> sx, cx, sy, cy;  // host copies
+    hm::DeviceBuffer table;              // {sx, cx, sy, cy} per turn
+    hm_arith arith = HM_ARITH_EXACT;
+};
+
+namespace hm {
+
+// ---- errors ---------------------------------------------------------------------
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<hm_cancel_fn> g_cancel_fn{nullptr};
+std::atomic<void *> g_cancel_ctx{nullptr};
+
+// Launch shape of the tracking kernels (set by the autotuner).
+struct TrackConfig {
+    int threads = 128;
+    int per_thread = 2;
+    uint32_t chunk0 = 512;      // turns of the first chunk
+    uint32_t chunk_max = 16384; // chunk length cap (chunks double up to it)
+};
+std::mutex g_cfg_mutex;
+TrackConfig g_cfg;
+
+TrackConfig track_config() {
+    std::lock_guard<std::mutex> lock(g_cfg_mutex);
+    return g_cfg;
+}
+
+// Kernel timing of the tracking launches (CUDA events on the launch stream).
+struct Profile {
+    std::atomic<bool> enabled{false};
+    std::mutex mutex;
+    double kernel_ms = 0.0;
+    uint64_t launches = 0;
+};
+Profile g_profile;
+
+// Event pair around one launch; elapsed time is added once the stream has
+// been synchronised.
+struct LaunchTimer {
+    cudaEvent_t start = nullptr, stop = nullptr;
+    bool armed = false;
+    ~LaunchTimer() {
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+    }
+    void begin(cudaStream_t s) {
+        if (!g_profile.enabled.load()) return;
+        if (!start) {
+            cudaEventCreate(&start);
+            cudaEventCreate(&stop);
+        }
+        cudaEventRecord(start, s);
+        armed = true;
+    }
+    void end(cudaStream_t s) {
+        if (armed) cudaEventRecord(stop, s);
+    }
+    void collect() {  // call after the stream has been synchronised
+        if (!armed) return;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, start, stop) == cudaSuccess) {
+            std::lock_guard<std::mutex> lock(g_profile.mutex);
+            g_profile.kernel_ms += ms;
+            g_profile.launches += 1;
+        }
+        armed = false;
+    }
+};
+}  // namespace
+
+hm_status fail(hm_status code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+hm_status ok() {
+    g_last_error.clear();
+    return HM_OK;
+}
+
+hm_status cuda_fail(cudaError_t err, const char *what) {
+    const hm_status code =
+        err == cudaErrorMemoryAllocation ? HM_ERR_OOM
+        : (err == cudaErrorNoDevice || err == cudaErrorInsufficientDriver) ? HM_ERR_NO_DEVICE
+                                                                           : HM_ERR_CUDA;
+    return fail(code, std::string("CUDA error: ") + cudaGetErrorString(err) + " (" + what + ")");
+}
+
+bool cancel_requested() {
+    hm_cancel_fn fn = g_cancel_fn.load();
+    return fn != nullptr && fn(g_cancel_ctx.load()) != 0;
+}
+
+// ---- device buffers ---------------------------------------------------------------
+
+DeviceBuffer &DeviceBuffer::operator=(DeviceBuffer &&o) noexcept {
+    if (this != &o) {
+        release();
+        ptr = o.ptr;
+        bytes = o.bytes;
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
+    return *this;
+}
+
+DeviceBuffer::~DeviceBuffer() { release(); }
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+hm_status DeviceBuffer::alloc(size_t nbytes) {
+    release();
+    if (nbytes == 0) return ok();
+    HM_CUDA_TRY(cudaMalloc(&ptr, nbytes));
+    bytes = nbytes;
+    return ok();
+}
+
+hm_status DeviceBuffer::ensure(size_t nbytes) {
+    if (nbytes <= bytes) return ok();
+    return alloc(nbytes);
+}
+
+// ---- chunked tracking driver --------------------------------------------------------
+
+namespace {
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct Workspace {
+    uint32_t *count[2];
+    uint32_t *idx[2];
+    double *x[2], *px[2], *y[2], *py[2];
+};
+
+Workspace carve(void *base, size_t n) {
+    Workspace w{};
+    char *p = static_cast<char *>(base);
+    w.count[0] = reinterpret_cast<uint32_t *>(p);
+    w.count[1] = w.count[0] + 1;
+    p += 256;
+    for (int b = 0; b < 2; ++b) {
+        w.idx[b] = reinterpret_cast<uint32_t *>(p);
+        p += align256(n * sizeof(uint32_t));
+        double **fields[4] = {&w.x[b], &w.px[b], &w.y[b], &w.py[b]};
+        for (double **f : fields) {
+            *f = reinterpret_cast<double *>(p);
+            p += align256(n * sizeof(double));
+        }
+    }
+    return w;
+}
+
+}  // namespace
+
+size_t track_workspace_bytes(size_t n) {
+    return 256 + 2 * (align256(n * sizeof(uint32_t)) + 4 * align256(n * sizeof(double)));
+}
+
+// Advances n particles by n_turns turns of the map; *turns_done receives
+// the turns actually applied (less than n_turns only when cancelled).
+hm_status track_driver(double *x, double *px, double *y, double *py,
+                       uint32_t *steps, size_t n, const double *table,
+                       uint64_t table_len, uint32_t s0, uint32_t n_turns,
+                       double mu, double barrier, bool inverse, hm_arith arith,
+                       void *workspace, cudaStream_t stream,
+                       uint32_t *turns_done) {
+    *turns_done = 0;
+    if (n == 0 || n_turns == 0) {
+        *turns_done = n_turns;  // nothing to move; the turn counter still advances
+        return ok();
+    }
+    if (n > 0xffffffffULL)
+        return fail(HM_ERR_INVALID_ARG, "too many particles for one launch list (max 2^32-1)");
+    if (!x || !px || !y || !py || !steps || !table)
+        return fail(HM_ERR_INVALID_ARG, "null device pointer");
+    if (arith != HM_ARITH_EXACT && arith != HM_ARITH_FAST)
+        return fail(HM_ERR_INVALID_ARG, "unknown arithmetic mode");
+    if (!inverse && uint64_t(s0) + n_turns > table_len)
+        return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    if (inverse && (n_turns > s0 || s0 > table_len))
+        return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+
+    const TrackConfig cfg = track_config();
+    const double b2 = barrier * barrier;
+    long long b2bits = 0;
+    if (!std::isnan(b2)) std::memcpy(&b2bits, &b2, sizeof(b2));
+
+    TrackChunk c{};
+    c.ux = x;
+    c.upx = px;
+    c.uy = y;
+    c.upy = py;
+    c.usteps = steps;
+    c.n_user = uint32_t(n);
+    c.table = table;
+    c.mu = mu;
+    c.b2bits = b2bits;
+    TrackLaunch l{int(arith), mu != 0.0, inverse, cfg.per_thread, cfg.threads};
+
+    const bool one_chunk = n_turns <= cfg.chunk0;
+    if (!one_chunk && workspace == nullptr)
+        return fail(HM_ERR_INVALID_ARG, "workspace required for more than one chunk of turns");
+    Workspace w{};
+    if (!one_chunk) w = carve(workspace, n);
+
+    uint32_t done = 0;
+    uint32_t chunk = cfg.chunk0;
+    uint32_t n_in = uint32_t(n);
+    int cur = -1;  // -1: the caller's arrays in identity order
+    LaunchTimer timer;
+    while (done < n_turns) {
+        const uint32_t len = std::min(chunk, n_turns - done);
+        const bool last = done + len == n_turns;
+        c.turn0 = inverse ? s0 - done : s0 + done;
+        c.n_turns = len;
+        c.steps_final = inverse ? s0 - (done + len) : s0 + (done + len);
+        if (cur < 0) {
+            c.in_idx = nullptr;
+            c.in_x = c.in_px = c.in_y = c.in_py = nullptr;
+            c.in_count = nullptr;
+        } else {
+            c.in_idx = w.idx[cur];
+            c.in_x = w.x[cur];
+            c.in_px = w.px[cur];
+            c.in_y = w.y[cur];
+            c.in_py = w.py[cur];
+            c.in_count = w.count[cur];
+        }
+        const int nxt = cur < 0 ? 0 : 1 - cur;
+        if (last) {
+            c.out_idx = nullptr;
+            c.out_count = nullptr;
+        } else {
+            c.out_idx = w.idx[nxt];
+            c.out_x = w.x[nxt];
+            c.out_px = w.px[nxt];
+            c.out_y = w.y[nxt];
+            c.out_py = w.py[nxt];
+            c.out_count = w.count[nxt];
+            HM_CUDA_TRY(cudaMemsetAsync(w.count[nxt], 0, sizeof(uint32_t), stream));
+        }
+        timer.begin(stream);
+        HM_CUDA_TRY(launch_track_chunk(c, l, n_in, stream));
+        timer.end(stream);
+        done += len;
+        chunk = std::min<uint32_t>(chunk * 2u, cfg.chunk_max);
+        if (last) break;
+        HM_CUDA_TRY(cudaMemcpyAsync(&n_in, w.count[nxt], sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, stream));
+        HM_CUDA_TRY(cudaStreamSynchronize(stream));
+        timer.collect();
+        cur = nxt;
+        if (n_in == 0) {
+            done = n_turns;  // every particle is lost; nothing left to write
+            break;
+        }
+        if (cancel_requested()) {
+            // Flush the survivors with their current steps and stop.
+            c.turn0 = inverse ? s0 - done : s0 + done;
+            c.n_turns = 0;
+            c.steps_final = c.turn0;
+            c.in_idx = w.idx[cur];
+            c.in_x = w.x[cur];
+            c.in_px = w.px[cur];
+            c.in_y = w.y[cur];
+            c.in_py = w.py[cur];
+            c.in_count = w.count[cur];
+            c.out_idx = nullptr;
+            c.out_count = nullptr;
+            HM_CUDA_TRY(launch_track_chunk(c, l, n_in, stream));
+            HM_CUDA_TRY(cudaStreamSynchronize(stream));
+            *turns_done = done;
+            return fail(HM_ERR_CANCELLED, "tracking cancelled");
+        }
+    }
+    HM_CUDA_TRY(cudaStreamSynchronize(stream));
+    timer.collect();
+    *turns_done = n_turns;
+    return ok();
+}
+
+hm_status set_profiling(int on) {
+    std::lock_guard<std::mutex> lock(g_profile.mutex);
+    g_profile.enabled.store(on != 0);
+    g_profile.kernel_ms = 0.0;
+    g_profile.launches = 0;
+    return ok();
+}
+
+hm_status get_profile(double *kernel_ms, uint64_t *launches) {
+    std::lock_guard<std::mutex> lock(g_profile.mutex);
+    if (kernel_ms) *kernel_ms = g_profile.kernel_ms;
+    if (launches) *launches = g_profile.launches;
+    return ok();
+}
+
+hm_status set_track_config(int threads, int per_thread, uint32_t chunk0, uint32_t chunk_max) {
+    if (threads < 32 || threads > 256 || threads % 32 != 0)
+        return fail(HM_ERR_INVALID_ARG, "threads must be 32..256 in steps of 32");
+    if (per_thread != 1 && per_thread != 2 && per_thread != 4)
+        return fail(HM_ERR_INVALID_ARG, "particles per thread must be 1, 2 or 4");
+    if (chunk0 == 0 || chunk_max < chunk0)
+        return fail(HM_ERR_INVALID_ARG, "need 0 < chunk0 <= chunk_max");
+    std::lock_guard<std::mutex> lock(g_cfg_mutex);
+    g_cfg = TrackConfig{threads, per_thread, chunk0, chunk_max};
+    return ok();
+}
+
+hm_status get_track_config(int *threads, int *per_thread, uint32_t *chunk0, uint32_t *chunk_max) {
+    const TrackConfig c = track_config();
+    if (threads) *threads = c.threads;
+    if (per_thread) *per_thread = c.per_thread;
+    if (chunk0) *chunk0 = c.chunk0;
+    if (chunk_max) *chunk_max = c.chunk_max;
+    return ok();
+}
+
+}  // namespace hm
+
+using hm::fail;
+using hm::ok;
+
+namespace {
+
+hm_status upload_tables(hm_tracker *t, const std::vector<double> &wx,
+                        const std::vector<double> &wy) {
+    const size_t n = wx.size();
+    t->sx.resize(n);
+    t->cx.resize(n);
+    t->sy.resize(n);
+    t->cy.resize(n);
+    // sin/cos of omega(n) with the host libm (src/henon.cu:2672-2686).
+    for (size_t i = 0; i < n; ++i) {
+        t->sx[i] = std::sin(wx[i]);
+        t->cx[i] = std::cos(wx[i]);
+        t->sy[i] = std::sin(wy[i]);
+        t->cy[i] = std::cos(wy[i]);
+    }
+    std::vector<double> rec(4 * n);
+    for (size_t i = 0; i < n; ++i) {
+        rec[4 * i + 0] = t->sx[i];
+        rec[4 * i + 1] = t->cx[i];
+        rec[4 * i + 2] = t->sy[i];
+        rec[4 * i + 3] = t->cy[i];
+    }
+    HM_TRY(t->table.alloc(rec.size() * sizeof(double)));
+    if (n) HM_CUDA_TRY(cudaMemcpy(t->table.ptr, rec.data(), rec.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice));
+    t->allowed_steps = n;
+    return ok();
+}
+
+hm_status compute_tables(hm_tracker *t, uint32_t n_turns, double omega_x, double omega_y,
+                         const char *kind, double omega_0, double epsilon, uint32_t offset) {
+    if (!kind) return fail(HM_ERR_INVALID_ARG, "null modulation kind");
+    std::vector<double> wx, wy;
+    HM_TRY(hm::modulation(kind, n_turns, omega_x, omega_y, omega_0, epsilon, offset, wx, wy));
+    return upload_tables(t, wx, wy);
+}
+
+hm_status particles_upload(hm_particles *p, const double *x, const double *px,
+                           const double *y, const double *py,
+                           const std::vector<uint32_t> &steps) {
+    const size_t n = p->n_total;
+    hm::DeviceBuffer *dbl[4] = {&p->x, &p->px, &p->y, &p->py};
+    const double *src[4] = {x, px, y, py};
+    for (int f = 0; f < 4; ++f) {
+        HM_TRY(dbl[f]->alloc(n * sizeof(double)));
+        if (n) HM_CUDA_TRY(cudaMemcpy(dbl[f]->ptr, src[f], n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    HM_TRY(p->steps.alloc(n * sizeof(uint32_t)));
+    HM_TRY(p->dvalid.alloc(n));
+    HM_TRY(p->dghost.alloc(n));
+    HM_TRY(p->didx.alloc(n * sizeof(uint64_t)));
+    HM_TRY(p->didx_base.alloc(n * sizeof(uint64_t)));
+    if (n) {
+        HM_CUDA_TRY(cudaMemcpy(p->steps.ptr, steps.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        HM_CUDA_TRY(cudaMemcpy(p->dvalid.ptr, p->valid.data(), n, cudaMemcpyHostToDevice));
+        HM_CUDA_TRY(cudaMemcpy(p->dghost.ptr, p->ghost.data(), n, cudaMemcpyHostToDevice));
+        HM_CUDA_TRY(cudaMemcpy(p->didx.ptr, p->idx.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        HM_CUDA_TRY(cudaMemcpy(p->didx_base.ptr, p->idx_base.data(), n * sizeof(uint64_t),
+                               cudaMemcpyHostToDevice));
+    }
+    return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *hm_last_error(void) { return hm::g_last_error.c_str(); }
+
+int hm_version(void) { return 10000; }
+
+int hm_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+hm_status hm_set_cancel_callback(hm_cancel_fn fn, void *ctx) {
+    hm::g_cancel_ctx.store(ctx);
+    hm::g_cancel_fn.store(fn);
+    return ok();
+}
+
+hm_status hm_set_track_config(int threads, int per_thread, uint32_t chunk0, uint32_t chunk_max) {
+    return hm::set_track_config(threads, per_thread, chunk0, chunk_max);
+}
+
+hm_status hm_get_track_config(int *threads, int *per_thread, uint32_t *chunk0, uint32_t *chunk_max) {
+    return hm::get_track_config(threads, per_thread, chunk0, chunk_max);
+}
+
+hm_status hm_set_profiling(int on) { return hm::set_profiling(on); }
+
+hm_status hm_get_profile(double *kernel_ms, uint64_t *launches) {
+    return hm::get_profile(kernel_ms, launches);
+}
+
+// ---- host numerics ----------------------------------------------------------------
+
+hm_status hm_modulation(const char *kind, uint32_t n_turns, double omega_x, double omega_y,
+                        double omega_0, double epsilon, uint32_t offset, double *omega_x_out,
+                        double *omega_y_out) {
+    if (!kind || (n_turns && (!omega_x_out || !omega_y_out)))
+        return fail(HM_ERR_INVALID_ARG, "null pointer");
+    std::vector<double> wx, wy;
+    HM_TRY(hm::modulation(kind, n_turns, omega_x, omega_y, omega_0, epsilon, offset, wx, wy));
+    std::memcpy(omega_x_out, wx.data(), wx.size() * sizeof(double));
+    std::memcpy(omega_y_out, wy.data(), wy.size() * sizeof(double));
+    return ok();
+}
+
+}  // extern "C"
+
+namespace hm {
+std::vector<double> sps_modulation(double tune, double epsilon, int32_t start, int32_t end);
+std::vector<double> basic_modulation(double tune, double omega, double epsilon, int32_t start,
+                                     int32_t end);
+}  // namespace hm
+
+extern "C" {
+
+hm_status hm_sps_modulation(double tune, double epsilon, int32_t start, int32_t end, double *out) {
+    if (start >= end) return fail(HM_ERR_INVALID_ARG, "sps_modulation needs start < end");
+    if (!out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    auto v = hm::sps_modulation(tune, epsilon, start, end);
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return ok();
+}
+
+hm_status hm_basic_modulation(double tune, double omega, double epsilon, int32_t start,
+                              int32_t end, double *out) {
+    if (start >= end) return fail(HM_ERR_INVALID_ARG, "basic_modulation needs start < end");
+    if (!out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    auto v = hm::basic_modulation(tune, omega, epsilon, start, end);
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+    return ok();
+}
+
+hm_status hm_birkhoff_weights(uint32_t n_weights, double *out) {
+    if (n_weights && !out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    auto w = hm::birkhoff_weights(n_weights);
+    std::memcpy(out, w.data(), w.size() * sizeof(double));
+    return ok();
+}
+
+// ---- tracker ----------------------------------------------------------------------
+
+hm_status hm_tracker_create(uint32_t n_turns, double omega_x, double omega_y,
+                            const char *modulation_kind, double omega_0, double epsilon,
+                            uint32_t offset, hm_tracker **out) {
+    if (!out) return fail(HM_ERR_INVALID_ARG, "null output handle");
+    *out = nullptr;
+    auto *t = new hm_tracker();
+    const hm_status s = compute_tables(t, n_turns, omega_x, omega_y, modulation_kind, omega_0,
+                                       epsilon, offset);
+    if (s != HM_OK) {
+        delete t;
+        return s;
+    }
+    *out = t;
+    return ok();
+}
+
+hm_status hm_tracker_compute_a_modulation(hm_tracker *t, uint32_t n_turns, double omega_x,
+                                          double omega_y, const char *modulation_kind,
+                                          double omega_0, double epsilon, uint32_t offset) {
+    if (!t) return fail(HM_ERR_INVALID_ARG, "null tracker");
+    return compute_tables(t, n_turns, omega_x, omega_y, modulation_kind, omega_0, epsilon, offset);
+}
+
+hm_status hm_tracker_destroy(hm_tracker *t) {
+    delete t;
+    return ok();
+}
+
+hm_status hm_tracker_allowed_steps(const hm_tracker *t, uint64_t *out) {
+    if (!t || !out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    *out = t->allowed_steps;
+    return ok();
+}
+
+hm_status hm_tracker_get_tables(const hm_tracker *t, double *sin_x, double *cos_x, double *sin_y,
+                                double *cos_y) {
+    if (!t) return fail(HM_ERR_INVALID_ARG, "null tracker");
+    const size_t n = t->sx.size();
+    if (n && (!sin_x || !cos_x || !sin_y || !cos_y)) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    std::memcpy(sin_x, t->sx.data(), n * sizeof(double));
+    std::memcpy(cos_x, t->cx.data(), n * sizeof(double));
+    std::memcpy(sin_y, t->sy.data(), n * sizeof(double));
+    std::memcpy(cos_y, t->cy.data(), n * sizeof(double));
+    return ok();
+}
+
+hm_status hm_tracker_device_tables(const hm_tracker *t, const double **out) {
+    if (!t || !out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    *out = t->table.as<const double>();
+    return ok();
+}
+
+hm_status hm_tracker_set_arith(hm_tracker *t, hm_arith arith) {
+    if (!t) return fail(HM_ERR_INVALID_ARG, "null tracker");
+    if (arith != HM_ARITH_EXACT && arith != HM_ARITH_FAST)
+        return fail(HM_ERR_INVALID_ARG, "unknown arithmetic mode");
+    t->arith = arith;
+    return ok();
+}
+
+hm_status hm_tracker_get_arith(const hm_tracker *t, hm_arith *out) {
+    if (!t || !out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    *out = t->arith;
+    return ok();
+}
+
+// ---- particles --------------------------------------------------------------------
+
+hm_status hm_particles_create(const double *x, const double *px, const double *y,
+                              const double *py, size_t n, hm_particles **out) {
+    if (!out) return fail(HM_ERR_INVALID_ARG, "null output handle");
+    *out = nullptr;
+    if (n && (!x || !px || !y || !py)) return fail(HM_ERR_INVALID_ARG, "null coordinate array");
+    if (n > 0xffffffffULL) return fail(HM_ERR_INVALID_ARG, "too many particles (max 2^32-1)");
+    auto *p = new hm_particles();
+    p->n_total = p->n_particles = n;
+    p->x0.assign(x, x + n);
+    p->px0.assign(px, px + n);
+    p->y0.assign(y, y + n);
+    p->py0.assign(py, py + n);
+    p->valid.assign(n, 1);
+    p->ghost.assign(n, 0);
+    p->idx.resize(n);
+    p->idx_base.resize(n);
+    for (size_t i = 0; i < n; ++i) p->idx[i] = p->idx_base[i] = i;
+    const hm_status s = particles_upload(p, x, px, y, py, std::vector<uint32_t>(n, 0u));
+    if (s != HM_OK) {
+        delete p;
+        return s;
+    }
+    *out = p;
+    return ok();
+}
+
+hm_status hm_particles_destroy(hm_particles *p) {
+    delete p;
+    return ok();
+}
+
+hm_status hm_particles_reset(hm_particles *p) {
+    if (!p) return fail(HM_ERR_INVALID_ARG, "null particles");
+    std::fill(p->valid.begin(), p->valid.end(), uint8_t(1));
+    p->live_step = 0;
+    return particles_upload(p, p->x0.data(), p->px0.data(), p->y0.data(), p->py0.data(),
+                            std::vector<uint32_t>(p->n_total, 0u));
+}
+
+hm_status hm_particles_size(const hm_particles *p, size_t *n_total, size_t *n_particles,
+                            size_t *n_ghosts) {
+    if (!p) return fail(HM_ERR_INVALID_ARG, "null particles");
+    if (n_total) *n_total = p->n_total;
+    if (n_particles) *n_particles = p->n_particles;
+    if (n_ghosts) *n_ghosts = p->n_ghosts;
+    return ok();
+}
+
+hm_status hm_particles_global_steps(const hm_particles *p, uint32_t *out) {
+    if (!p || !out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    *out = p->global_steps;
+    return ok();
+}
+
+hm_status hm_particles_device_ptr(const hm_particles *p, hm_field field, void **out) {
+    if (!p || !out) return fail(HM_ERR_INVALID_ARG, "null pointer");
+    switch (field) {
+        case HM_FIELD_X: *out = p->x.ptr; break;
+        case HM_FIELD_PX: *out = p->px.ptr; break;
+        case HM_FIELD_Y: *out = p->y.ptr; break;
+        case HM_FIELD_PY: *out = p->py.ptr; break;
+        case HM_FIELD_STEPS: *out = p->steps.ptr; break;
+        case HM_FIELD_VALID: *out = p->dvalid.ptr; break;
+        case HM_FIELD_GHOST: *out = p->dghost.ptr; break;
+        case HM_FIELD_IDX: *out = p->didx.ptr; break;
+        case HM_FIELD_IDX_BASE: *out = p->didx_base.ptr; break;
+        default: return fail(HM_ERR_INVALID_ARG, "unknown field");
+    }
+    return ok();
+}
+
+hm_status hm_particles_get(const hm_particles *p, hm_field field, void *host_out) {
+    if (!p) return fail(HM_ERR_INVALID_ARG, "null particles");
+    void *src = nullptr;
+    HM_TRY(hm_particles_device_ptr(p, field, &src));
+    size_t elem = 8;
+    if (field == HM_FIELD_STEPS) elem = 4;
+    if (field == HM_FIELD_VALID || field == HM_FIELD_GHOST) elem = 1;
+    const size_t bytes = p->n_total * elem;
+    if (bytes == 0) return ok();
+    if (!host_out) return fail(HM_ERR_INVALID_ARG, "null output");
+    HM_CUDA_TRY(cudaMemcpy(host_out, src, bytes, cudaMemcpyDeviceToHost));
+    return ok();
+}
+
+hm_status hm_particles_observable(const hm_particles *p, hm_observable kind, double *host_out) {
+    if (!p) return fail(HM_ERR_INVALID_ARG, "null particles");
+    if (kind < HM_OBS_RADIUS || kind > HM_OBS_ANGLE_Y) return fail(HM_ERR_INVALID_ARG, "unknown observable");
+    const size_t n = p->n_total;
+    if (n == 0) return ok();
+    if (!host_out) return fail(HM_ERR_INVALID_ARG, "null output");
+    hm::DeviceBuffer out;
+    HM_TRY(out.alloc(n * sizeof(double)));
+    HM_CUDA_TRY(hm::launch_observable(p->x.as<double>(), p->px.as<double>(), p->y.as<double>(),
+                                      p->py.as<double>(), out.as<double>(), n, int(kind), 0));
+    HM_CUDA_TRY(cudaMemcpy(host_out, out.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return ok();
+}
+
+// ---- tracking ---------------------------------------------------------------------
+
+size_t hm_track_workspace_bytes(size_t n) { return hm::track_workspace_bytes(n); }
+
+hm_status hm_track_device(double *x, double *px, double *y, double *py, uint32_t *steps, size_t n,
+                          const double *tables, uint64_t table_len, uint32_t start_step,
+                          uint32_t n_turns, double mu, double barrier, int inverse,
+                          hm_arith arith, void *workspace, void *stream) {
+    uint32_t done = 0;
+    return hm::track_driver(x, px, y, py, steps, n, tables, table_len, start_step, n_turns, mu,
+                            barrier, inverse != 0, arith, workspace,
+                            static_cast<cudaStream_t>(stream), &done);
+}
+
+hm_status hm_track(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu, double barrier,
+                   double kick_module, int inverse) {
+    if (!t || !p) return fail(HM_ERR_INVALID_ARG, "null tracker or particles");
+    // Turn budget (src/henon.cu:3158-3167), in 64-bit arithmetic.
+    if (inverse) {
+        if (n_turns > p->global_steps) return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    } else {
+        if (uint64_t(n_turns) + p->global_steps > t->allowed_steps)
+            return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    }
+    if (!std::isnan(kick_module))
+        return fail(HM_ERR_NOT_SUPPORTED, "random kicks (kick_module) are not provided by this build");
+    if (inverse && n_turns > p->live_step)
+        return fail(HM_ERR_BUDGET,
+                    "The number of turns is too large. (inverse tracking past the particles' steps)");
+    void *ws = nullptr;
+    if (p->n_total) {
+        HM_TRY(p->work.ensure(hm::track_workspace_bytes(p->n_total)));
+        ws = p->work.ptr;
+    }
+    uint32_t done = 0;
+    const hm_status s = hm::track_driver(
+        p->x.as<double>(), p->px.as<double>(), p->y.as<double>(), p->py.as<double>(),
+        p->steps.as<uint32_t>(), p->n_total, t->table.as<const double>(), t->allowed_steps,
+        p->live_step, n_turns, mu, barrier, inverse != 0, t->arith, ws, 0, &done);
+    if (s != HM_OK && s != HM_ERR_CANCELLED) return s;
+    // global_steps follows the turns applied (src/henon.cu:3181-3184).
+    if (inverse) {
+        p->global_steps -= done;
+        p->live_step -= done;
+    } else {
+        p->global_steps += done;
+        p->live_step += done;
+    }
+    return s;
+}
+
+// ---- measurement -------------------------------------------------------------------
+
+hm_status hm_fp64_peak(double seconds_target, double *tflops, double *ms) {
+    if (!tflops) return fail(HM_ERR_INVALID_ARG, "null output");
+    int dev = 0, sms = 0;
+    HM_CUDA_TRY(cudaGetDevice(&dev));
+    HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    hm::DeviceBuffer sink;
+    HM_TRY(sink.alloc(size_t(sms) * 64 * sizeof(double)));
+    cudaEvent_t a, b;
+    HM_CUDA_TRY(cudaEventCreate(&a));
+    HM_CUDA_TRY(cudaEventCreate(&b));
+    const int blocks = sms * 8, threads = 256;
+    int iters = 256;
+    double flops = 0.0;
+    float elapsed = 0.f;
+    // Warm up, then grow the launch until it lasts about seconds_target.
+    for (int round = 0; round < 12; ++round) {
+        HM_CUDA_TRY(cudaEventRecord(a, 0));
+        HM_CUDA_TRY(hm::launch_fp64_peak(sink.as<double>(), blocks, threads, iters, 0, &flops));
+        HM_CUDA_TRY(cudaEventRecord(b, 0));
+        HM_CUDA_TRY(cudaEventSynchronize(b));
+        HM_CUDA_TRY(cudaEventElapsedTime(&elapsed, a, b));
+        if (round > 0 && elapsed * 1e-3 >= seconds_target) break;
+        if (elapsed * 1e-3 < seconds_target) {
+            const double scale = elapsed > 0.f ? seconds_target / (elapsed * 1e-3) : 8.0;
+            iters = int(std::min(double(iters) * std::min(scale * 1.1, 8.0), 1e8));
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *tflops = flops / (double(elapsed) * 1e-3) / 1e12;
+    if (ms) *ms = elapsed;
+    return ok();
+}
+
+}  // extern "C"

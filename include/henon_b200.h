@@ -1,0 +1,209 @@
+/*
+ * henon_b200.h -- C ABI of the B200-native Henon-map tracking library
+ * (libhenon_b200.so).
+ *
+ * Every entry point takes plain pointers and sizes, returns an hm_status and
+ * never exits the process.  The message of the last failure on the calling
+ * thread is available from hm_last_error().
+ *
+ * Reference interfaces replaced (paths inside carlidel/henon_map_cpp):
+ *   - src/bind.cpp:224-578      pybind11 module `henon_map_engine`
+ *   - src/henon.h:41-447        particles_4d[_gpu], henon_tracker[_gpu], the
+ *                               tangent-map, indicator and storage classes
+ *   - src/modulation.h:12-22    modulation tables
+ *   - src/dynamic_indicator.h   birkhoff_weights
+ *
+ * Device memory layout (HBM):
+ *   particles : structure of arrays, double x[n], px[n], y[n], py[n],
+ *               uint32 steps[n], uint8 valid[n], uint8 ghost[n],
+ *               uint64 idx[n], idx_base[n]   (n includes ghost particles)
+ *   tracker   : one 32-byte record per turn {sin wx, cos wx, sin wy, cos wy}
+ *               so that a chunk of turns is one contiguous bulk copy.
+ *   matrices  : double[n][16] row-major 4x4 per particle (as the reference).
+ *   vectors   : double[n][4].
+ */
+#ifndef HENON_B200_H
+#define HENON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hm_status {
+    HM_OK = 0,
+    HM_ERR_INVALID_ARG = 1,        /* bad size, pointer or option            */
+    HM_ERR_BUDGET = 2,             /* "The number of turns is too large."    */
+    HM_ERR_CUDA = 3,               /* a CUDA runtime call failed             */
+    HM_ERR_TIMEOUT = 4,            /* a bounded device wait gave up          */
+    HM_ERR_CANCELLED = 5,          /* the cancel callback asked to stop      */
+    HM_ERR_OOM = 6,                /* device allocation failed               */
+    HM_ERR_UNKNOWN_MODULATION = 7, /* "Unknown modulation kind"              */
+    HM_ERR_NOT_SUPPORTED = 8,      /* option not provided by this build      */
+    HM_ERR_NO_DEVICE = 9           /* no CUDA device visible                 */
+} hm_status;
+
+/* Arithmetic of the map kernels.
+ * HM_ARITH_EXACT: every multiply and add is a separately rounded IEEE-754
+ *   binary64 operation in the reference's operation order (no contraction to
+ *   FMA) -- results are bit-identical to the reference CPU path and to the
+ *   reference CUDA path built with --fmad=false.
+ * HM_ARITH_FAST: fused multiply-adds and reassociated polynomials; agrees
+ *   with EXACT to rounding error per turn. */
+typedef enum hm_arith { HM_ARITH_EXACT = 0, HM_ARITH_FAST = 1 } hm_arith;
+
+/* Particle fields for hm_particles_get (host copies, like the reference's
+ * getters, src/henon.cu:1444-1482, 1646-1676). */
+typedef enum hm_field {
+    HM_FIELD_X = 0,        /* double  */
+    HM_FIELD_PX = 1,       /* double  */
+    HM_FIELD_Y = 2,        /* double  */
+    HM_FIELD_PY = 3,       /* double  */
+    HM_FIELD_STEPS = 4,    /* uint32  */
+    HM_FIELD_VALID = 5,    /* uint8   */
+    HM_FIELD_GHOST = 6,    /* uint8   */
+    HM_FIELD_IDX = 7,      /* uint64  */
+    HM_FIELD_IDX_BASE = 8  /* uint64  */
+} hm_field;
+
+/* Elementwise observables (src/henon.cu:67-111 and 979-1121). */
+typedef enum hm_observable {
+    HM_OBS_RADIUS = 0,     /* sqrt(x^2+px^2+y^2+py^2) */
+    HM_OBS_ACTION = 1,     /* x^2+px^2+y^2+py^2        */
+    HM_OBS_ACTION_X = 2,   /* x^2+px^2                 */
+    HM_OBS_ACTION_Y = 3,   /* y^2+py^2                 */
+    HM_OBS_ANGLE_X = 4,    /* atan2(px, x)             */
+    HM_OBS_ANGLE_Y = 5     /* atan2(py, y)             */
+} hm_observable;
+
+typedef struct hm_particles hm_particles;
+typedef struct hm_tracker hm_tracker;
+
+/* ---- library ----------------------------------------------------------- */
+
+/* Message of the last failure on this thread ("" if none). */
+const char *hm_last_error(void);
+/* ABI version of this library (major * 10000 + minor * 100 + patch). */
+int hm_version(void);
+/* Number of CUDA devices visible (0 when none); never fails. */
+int hm_device_count(void);
+
+/* Called between turn chunks of every long operation; a non-zero return
+ * stops the operation with HM_ERR_CANCELLED after the state has been made
+ * consistent (replaces check_keyboard_interrupt, src/henon.cu:7-15). */
+typedef int (*hm_cancel_fn)(void *ctx);
+hm_status hm_set_cancel_callback(hm_cancel_fn fn, void *ctx);
+
+/* Launch shape of the chunked tracking kernels: threads per block (32..256,
+ * multiple of 32), particles per thread (1, 2 or 4), turns of the first
+ * chunk and the cap of the doubling chunk length.  Process-wide; chosen by
+ * the autotuner.  Results do not depend on it. */
+hm_status hm_set_track_config(int threads, int per_thread, uint32_t chunk0,
+                              uint32_t chunk_max);
+hm_status hm_get_track_config(int *threads, int *per_thread,
+                              uint32_t *chunk0, uint32_t *chunk_max);
+
+/* ---- host numerics ----------------------------------------------------- */
+
+/* omega(n) for n in [offset, offset+n_turns) for both planes.
+ * kind: "sps", "basic", "none", "gaussian", "uniform"
+ * (pick_a_modulation, src/modulation.cpp:101-134; "none" fills the constant
+ * omega, see the library documentation). */
+hm_status hm_modulation(const char *kind, uint32_t n_turns, double omega_x,
+                        double omega_y, double omega_0, double epsilon,
+                        uint32_t offset, double *omega_x_out,
+                        double *omega_y_out);
+/* sps_modulation, src/modulation.cpp:31-60 (start < end). */
+hm_status hm_sps_modulation(double tune, double epsilon, int32_t start,
+                            int32_t end, double *out);
+/* basic_modulation, src/modulation.cpp:3-11 (start < end). */
+hm_status hm_basic_modulation(double tune, double omega, double epsilon,
+                              int32_t start, int32_t end, double *out);
+/* birkhoff_weights, src/dynamic_indicator.cpp:63-79. */
+hm_status hm_birkhoff_weights(uint32_t n_weights, double *out);
+
+/* ---- tracker (henon_tracker_gpu, src/henon.cu:3114-3185) --------------- */
+
+hm_status hm_tracker_create(uint32_t n_turns, double omega_x, double omega_y,
+                            const char *modulation_kind, double omega_0,
+                            double epsilon, uint32_t offset, hm_tracker **out);
+/* henon_tracker_gpu::compute_a_modulation, src/henon.cu:3135-3153. */
+hm_status hm_tracker_compute_a_modulation(hm_tracker *t, uint32_t n_turns,
+                                          double omega_x, double omega_y,
+                                          const char *modulation_kind,
+                                          double omega_0, double epsilon,
+                                          uint32_t offset);
+hm_status hm_tracker_destroy(hm_tracker *t);
+/* Turns the tables hold (allowed_steps in the reference). */
+hm_status hm_tracker_allowed_steps(const hm_tracker *t, uint64_t *out);
+/* Host copies of the four tables, each of allowed_steps doubles. */
+hm_status hm_tracker_get_tables(const hm_tracker *t, double *sin_x,
+                                double *cos_x, double *sin_y, double *cos_y);
+/* Device pointer to the interleaved {sx,cx,sy,cy} turn records. */
+hm_status hm_tracker_device_tables(const hm_tracker *t, const double **out);
+hm_status hm_tracker_set_arith(hm_tracker *t, hm_arith arith);
+hm_status hm_tracker_get_arith(const hm_tracker *t, hm_arith *out);
+
+/* ---- particles (particles_4d_gpu, src/henon.cu:1154-1691) -------------- */
+
+hm_status hm_particles_create(const double *x, const double *px,
+                              const double *y, const double *py, size_t n,
+                              hm_particles **out);
+hm_status hm_particles_destroy(hm_particles *p);
+/* particles_4d::reset, src/henon.cu:727-735 (global_steps is kept). */
+hm_status hm_particles_reset(hm_particles *p);
+/* Total size including ghosts, base particle count, ghosts per particle. */
+hm_status hm_particles_size(const hm_particles *p, size_t *n_total,
+                            size_t *n_particles, size_t *n_ghosts);
+hm_status hm_particles_global_steps(const hm_particles *p, uint32_t *out);
+/* Host copy of one field (n_total elements of the field's type). */
+hm_status hm_particles_get(const hm_particles *p, hm_field field,
+                           void *host_out);
+/* Device pointer of one field (valid until the next add_ghost/destroy). */
+hm_status hm_particles_device_ptr(const hm_particles *p, hm_field field,
+                                  void **out);
+/* Elementwise observable of all n_total entries (GPU getters). */
+hm_status hm_particles_observable(const hm_particles *p, hm_observable kind,
+                                  double *host_out);
+
+/* ---- tracking ---------------------------------------------------------- */
+
+/* henon_tracker_gpu::track, src/henon.cu:3155-3185: n_turns turns of the
+ * map on every particle, fused into chunked multi-turn launches.
+ * kick_module must be NaN (random kicks are not provided). */
+hm_status hm_track(hm_tracker *t, hm_particles *p, uint32_t n_turns,
+                   double mu, double barrier, double kick_module, int inverse);
+
+/* Kernel-level form of the same operation on caller-owned device arrays
+ * (the loop body of gpu_henon_track, src/henon.cu:636-691).  start_step is
+ * the steps value shared by all live particles; tables holds table_len
+ * records.  workspace must hold hm_track_workspace_bytes(n) bytes of device
+ * memory (NULL is allowed when n_turns fits one chunk).  stream is a
+ * cudaStream_t (NULL = legacy default stream).  Synchronous. */
+size_t hm_track_workspace_bytes(size_t n);
+hm_status hm_track_device(double *x, double *px, double *y, double *py,
+                          uint32_t *steps, size_t n, const double *tables,
+                          uint64_t table_len, uint32_t start_step,
+                          uint32_t n_turns, double mu, double barrier,
+                          int inverse, hm_arith arith, void *workspace,
+                          void *stream);
+
+/* ---- measurement ------------------------------------------------------- */
+
+/* Times every tracking kernel launch with CUDA events on its stream while
+ * enabled (turning it on or off resets the totals). */
+hm_status hm_set_profiling(int on);
+/* Summed device time (ms) and number of timed tracking launches. */
+hm_status hm_get_profile(double *kernel_ms, uint64_t *launches);
+
+/* FP64 FMA-chain microbenchmark on the current device: *tflops receives
+ * the achieved FP64 rate (an FMA counts as 2 flops). */
+hm_status hm_fp64_peak(double seconds_target, double *tflops, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HENON_B200_H */

@@ -1,0 +1,173 @@
+"""Python access to the CPU oracle (oracle/henon_oracle.c) and to the
+reference build (oracle/_ref/).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the library.
+
+The C restatement follows the reference's arithmetic line by line (each C
+function cites the reference file:line).  It is pinned two ways:
+  * against golden values recorded in the reference's own notebooks
+    (tests/golden/notebook_values.json), and
+  * bit for bit against the reference itself, built from its sources by
+    oracle/build_ref.sh, on seeded inputs (tests/golden/ref_track_*.npz,
+    made by tests/golden/make_golden.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib.util
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+SRC = HERE / "henon_oracle.c"
+REF_DIR = HERE / "_ref"
+
+_D = ctypes.c_double
+_PD = ctypes.POINTER(ctypes.c_double)
+_PU32 = ctypes.POINTER(ctypes.c_uint32)
+
+
+def build(force: bool = False) -> Path:
+    """Compiles the C restatement (no FMA contraction, no -march)."""
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < SRC.stat().st_mtime:
+        cmd = ["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-ffp-contract=off",
+               "-fno-fast-math", "-fopenmp", str(SRC), "-o", str(LIB_PATH), "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.or_sps_modulation.argtypes = [_D, _D, ctypes.c_int32, ctypes.c_int32, _PD]
+        L.or_basic_modulation.argtypes = [_D, _D, _D, ctypes.c_int32, ctypes.c_int32, _PD]
+        L.or_tables.argtypes = [_PD, ctypes.c_size_t, _PD, _PD]
+        L.or_birkhoff_weights.argtypes = [ctypes.c_uint32, _PD]
+        L.or_track.argtypes = [_PD, _PD, _PD, _PD, _PU32, ctypes.c_size_t, _PD, _PD, _PD, _PD,
+                               ctypes.c_uint32, _D, _D, ctypes.c_int, ctypes.c_int]
+        L.or_max_threads.restype = ctypes.c_int
+        L.or_tangent_matrix.argtypes = [_D] * 9 + [_PD]
+        L.or_matmul4.argtypes = [_PD, _PD, _PD]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray, ct=_PD):
+    return a.ctypes.data_as(ct)
+
+
+def max_threads() -> int:
+    return int(lib().or_max_threads())
+
+
+# ---- modulation -------------------------------------------------------------
+
+def sps_modulation(tune: float, epsilon: float, start: int, end: int) -> np.ndarray:
+    out = np.empty(end - start, dtype=np.float64)
+    lib().or_sps_modulation(tune, epsilon, start, end, _p(out))
+    return out
+
+
+def basic_modulation(tune: float, omega: float, epsilon: float, start: int, end: int) -> np.ndarray:
+    out = np.empty(end - start, dtype=np.float64)
+    lib().or_basic_modulation(tune, omega, epsilon, start, end, _p(out))
+    return out
+
+
+def omegas(n_turns: int, omega_x: float, omega_y: float, kind: str = "sps",
+           omega_0: float = float("nan"), epsilon: float = 0.0, offset: int = 0):
+    """pick_a_modulation (src/modulation.cpp:101-134) for the deterministic kinds."""
+    if kind == "sps":
+        return (sps_modulation(omega_x, epsilon, offset, offset + n_turns),
+                sps_modulation(omega_y, epsilon, offset, offset + n_turns))
+    if kind == "basic":
+        return (basic_modulation(omega_x, omega_0, epsilon, offset, offset + n_turns),
+                basic_modulation(omega_y, omega_0, epsilon, offset, offset + n_turns))
+    raise ValueError(f"oracle has no deterministic modulation '{kind}'")
+
+
+def tables(n_turns: int, omega_x: float, omega_y: float, kind: str = "sps",
+           omega_0: float = float("nan"), epsilon: float = 0.0, offset: int = 0):
+    """(sin wx, cos wx, sin wy, cos wy) with libm, as henon.cu:2679-2682."""
+    wx, wy = omegas(n_turns, omega_x, omega_y, kind, omega_0, epsilon, offset)
+    out = [np.empty(n_turns) for _ in range(4)]
+    lib().or_tables(_p(wx), n_turns, _p(out[0]), _p(out[1]))
+    lib().or_tables(_p(wy), n_turns, _p(out[2]), _p(out[3]))
+    return tuple(out)
+
+
+def birkhoff_weights(n: int) -> np.ndarray:
+    out = np.empty(n, dtype=np.float64)
+    lib().or_birkhoff_weights(n, _p(out))
+    return out
+
+
+# ---- tracking -----------------------------------------------------------------
+
+def track(x, px, y, py, steps, tabs, n_turns: int, mu: float, barrier: float,
+          inverse: bool = False, n_threads: int = 0):
+    """henon_tracker::track (src/henon.cu:2701-2752) on copies of the inputs.
+
+    Returns (x, px, y, py, steps) after n_turns turns."""
+    x = np.array(x, dtype=np.float64, copy=True)
+    px = np.array(px, dtype=np.float64, copy=True)
+    y = np.array(y, dtype=np.float64, copy=True)
+    py = np.array(py, dtype=np.float64, copy=True)
+    steps = np.array(steps, dtype=np.uint32, copy=True)
+    sx, cx, sy, cy = (np.ascontiguousarray(t, dtype=np.float64) for t in tabs)
+    lib().or_track(_p(x), _p(px), _p(y), _p(py), _p(steps, _PU32), x.size,
+                   _p(sx), _p(cx), _p(sy), _p(cy), n_turns, mu, barrier,
+                   int(bool(inverse)), int(n_threads))
+    return x, px, y, py, steps
+
+
+def tangent_matrix(x, px, y, py, sx, cx, sy, cy, mu) -> np.ndarray:
+    out = np.empty(16)
+    lib().or_tangent_matrix(x, px, y, py, sx, cx, sy, cy, mu, _p(out))
+    return out.reshape(4, 4)
+
+
+def matmul4(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.empty(16)
+    lib().or_matmul4(_p(a), _p(b), _p(out))
+    return out.reshape(4, 4)
+
+
+# ---- the reference build ------------------------------------------------------
+
+def reference_module(variant: str = "fmad_off"):
+    """Imports oracle/_ref/<variant>/henon_map_engine (the unmodified
+    reference, built by oracle/build_ref.sh), or returns None when absent."""
+    d = REF_DIR / variant
+    cands = sorted(d.glob("henon_map_engine*.so")) if d.exists() else []
+    if not cands:
+        return None
+    name = f"_hm_reference_{variant}"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location("henon_map_engine", cands[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    sys.modules[name] = mod
+    return mod
+
+
+def build_reference() -> bool:
+    """Runs oracle/build_ref.sh when the reference sources are present."""
+    if not Path(os.environ.get("REF", "/root/reference"), "src").exists():
+        return False
+    subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True)
+    return True

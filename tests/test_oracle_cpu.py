@@ -1,0 +1,84 @@
+"""Pins the CPU oracle before anything is checked against it.
+
+1. Against the golden fixtures made by running the reference itself
+   (tests/golden/ref_*.npz, tests/golden/make_golden.py): bit for bit.
+2. Against known answers recorded in the reference's notebooks
+   (tests/golden/notebook_values.json): to their printed precision.
+3. Against the reference build live when oracle/_ref/ is present.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import NAN, TUNES, assert_bitwise, golden_json, golden_npz, grid
+from oracle import oracle as O
+
+CASES = ["c1_like", "eps16_mu02", "eps64_mu02", "eps1_mu0", "eps32_mum05"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_track_equals_reference_fixture(case):
+    g = golden_npz(f"ref_track_{case}.npz")
+    nt = int(g["n_turns"])
+    tabs = O.tables(nt, *g["tunes"], "sps", epsilon=float(g["epsilon"]))
+    got = O.track(g["x0"], g["px0"], g["y0"], g["py0"], np.zeros(g["x0"].size, np.uint32),
+                  tabs, nt, float(g["mu"]), 10.0)
+    for a, k in zip(got[:4], ("x", "px", "y", "py")):
+        assert_bitwise(a, g[k], k)
+    np.testing.assert_array_equal(got[4], g["steps"])
+
+
+def test_oracle_reverse_equals_reference_fixture():
+    g = golden_npz("ref_reverse.npz")
+    tabs = O.tables(1000, *g["tunes"], "sps", epsilon=64.0)
+    f = O.track(g["x0"], g["px0"], g["y0"], g["py0"], np.zeros(200, np.uint32), tabs, 1000,
+                0.1, 10.0)
+    for a, k in zip(f, ("fx", "fpx", "fy", "fpy", "fsteps")):
+        assert_bitwise(a, g[k], k) if a.dtype == np.float64 else np.testing.assert_array_equal(a, g[k])
+    b = O.track(*f, tabs, 1000, 0.1, 10.0, inverse=True)
+    for a, k in zip(b, ("bx", "bpx", "by", "bpy", "bsteps")):
+        assert_bitwise(a, g[k], k) if a.dtype == np.float64 else np.testing.assert_array_equal(a, g[k])
+
+
+def test_oracle_modulation_equals_reference_fixture():
+    g = golden_npz("ref_modulation.npz")
+    assert_bitwise(O.sps_modulation(TUNES[0], 16.0, 0, 4000), g["sps_x_eps16"])
+    assert_bitwise(O.sps_modulation(TUNES[1], 64.0, 12345, 12345 + 3000), g["sps_y_eps64_off"])
+    assert_bitwise(O.basic_modulation(0.31, 0.01, 0.5, 0, 2000), g["basic_x"])
+    assert_bitwise(O.birkhoff_weights(10), g["bw10"])
+    assert_bitwise(O.birkhoff_weights(1000), g["bw1000"])
+
+
+def test_oracle_notebook_known_answers():
+    nb = golden_json("notebook_values.json")
+    sx, cx, sy, cy = O.tables(1000, *TUNES, "sps", epsilon=0.0)
+    m0 = O.tangent_matrix(0.1, 0.0, 0.1, 0.0, sx[0], cx[0], sy[0], cy[0], 0.0)
+    np.testing.assert_allclose(m0, nb["tangent_matrix_x0"]["matrix"], rtol=1e-7, atol=1e-8)
+    x1 = O.track([0.1], [0.0], [0.1], [0.0], [0], (sx, cx, sy, cy), 1, 0.0, 10.0)
+    np.testing.assert_allclose(x1[0][0], nb["x_after_one_turn"]["value"], rtol=1e-7)
+    m1 = O.tangent_matrix(x1[0][0], x1[1][0], x1[2][0], x1[3][0], sx[1], cx[1], sy[1], cy[1], 0.0)
+    np.testing.assert_allclose(m1, nb["tangent_matrix_x1"]["matrix"], rtol=1e-7, atol=1e-8)
+    np.testing.assert_allclose(O.birkhoff_weights(10), nb["birkhoff_weights_10"]["value"],
+                               rtol=1e-7, atol=1e-12)
+    v = m0 @ np.array([1.0, 0.0, 0.0, 0.0])
+    vm = nb["vector_multiply_normalize"]
+    np.testing.assert_allclose(v, vm["multiplied"], rtol=1e-7)
+    np.testing.assert_allclose(np.log(np.linalg.norm(v)), vm["log_norm"], rtol=1e-12)
+
+
+@pytest.mark.skipif(O.reference_module("fmad_off") is None, reason="reference build absent")
+@pytest.mark.parametrize("eps,mu,nt", [(0.0, 0.0, 1500), (16.0, 0.2, 1500), (64.0, -0.3, 1200)])
+def test_oracle_equals_reference_build_live(eps, mu, nt):
+    R = O.reference_module("fmad_off")
+    x, px, y, py = grid(0.55, 20, px0=0.001)
+    t = R.henon_tracker(nt, *TUNES, "sps", NAN, eps, 0)
+    p = R.particles_4d(x, px, y, py)
+    t.track(p, nt, mu, 10.0)
+    want = [np.asarray(p.get_x()), np.asarray(p.get_px()), np.asarray(p.get_y()),
+            np.asarray(p.get_py()), np.asarray(p.get_steps())]
+    got = O.track(x, px, y, py, np.zeros(x.size, np.uint32),
+                  O.tables(nt, *TUNES, "sps", epsilon=eps), nt, mu, 10.0)
+    for a, b in zip(got[:4], want[:4]):
+        assert_bitwise(a, b)
+    np.testing.assert_array_equal(got[4], want[4])
