@@ -31,7 +31,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
              f"-I{CUDA_HOME / 'include'}", f"-I{INCLUDE}"]
 
-CU_SOURCES = ["track.cu"]
+CU_SOURCES = ["track.cu", "noalloc.cu"]
 CPP_SOURCES = ["capi.cpp", "modulation.cpp"]
 
 

@@ -168,8 +168,6 @@ hm_status DeviceBuffer::ensure(size_t nbytes) {
 
 namespace {
 
-size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
-
 struct Workspace {
     uint32_t *count[2];
     uint32_t *idx[2];
@@ -195,10 +193,6 @@ Workspace carve(void *base, size_t n) {
 }
 
 }  // namespace
-
-size_t track_workspace_bytes(size_t n) {
-    return 256 + 2 * (align256(n * sizeof(uint32_t)) + 4 * align256(n * sizeof(double)));
-}
 
 // Advances n particles by n_turns turns of the map; *turns_done receives
 // the turns actually applied (less than n_turns only when cancelled).

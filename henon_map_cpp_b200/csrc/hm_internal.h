@@ -105,6 +105,23 @@ struct TrackLaunch {
 cudaError_t launch_track_chunk(const TrackChunk &c, const TrackLaunch &l,
                                uint32_t n_in_upper, cudaStream_t s);
 
+// Scratch layout of the chunked tracker for n particles: 256 bytes of
+// counters, then two survivor lists of {uint32 idx, double x, px, y, py}.
+constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+constexpr size_t track_workspace_bytes(size_t n) {
+    return 256 + 2 * (align256(n * sizeof(uint32_t)) + 4 * align256(n * sizeof(double)));
+}
+
+// Host driver of the chunked tracking launches (capi.cpp).  `workspace`
+// holds track_workspace_bytes(n) bytes of device memory (may be null when
+// n_turns fits one chunk); *turns_done receives the turns applied.
+hm_status track_driver(double *x, double *px, double *y, double *py,
+                       uint32_t *steps, size_t n, const double *table,
+                       uint64_t table_len, uint32_t s0, uint32_t n_turns,
+                       double mu, double barrier, bool inverse, hm_arith arith,
+                       void *workspace, cudaStream_t stream,
+                       uint32_t *turns_done);
+
 // Elementwise observable kernel launcher.
 cudaError_t launch_observable(const double *x, const double *px,
                               const double *y, const double *py, double *out,

@@ -190,6 +190,26 @@ hm_status hm_track_device(double *x, double *px, double *y, double *py,
                           int inverse, hm_arith arith, void *workspace,
                           void *stream);
 
+/* No counterpart in the reference.  The same operation as hm_track_device
+ * for callers that cannot allocate device memory (an application that
+ * reserves all device memory at start-up, a framework whose allocator owns
+ * every device byte, a loop that cannot take cudaFree's device-wide
+ * synchronisation): it calls no cudaMalloc, cudaFree or allocating library
+ * routine.  Its scratch is a fixed device array built into the library
+ * (room for HM_NOALLOC_MAX_PARTICLES particles, about 9 MiB, held by every
+ * GPU that loads the library until the process exits); n above that limit
+ * is rejected with HM_ERR_INVALID_ARG.  The first call on each device looks
+ * up the array's device address (cudaGetSymbolAddress), so make that first
+ * call before any stream capture.  All calls on a device share the array:
+ * calls that overlap on the GPU race.  Synchronous. */
+#define HM_NOALLOC_MAX_PARTICLES 131072u
+hm_status hm_track_device_noalloc(double *x, double *px, double *y, double *py,
+                                  uint32_t *steps, size_t n,
+                                  const double *tables, uint64_t table_len,
+                                  uint32_t start_step, uint32_t n_turns,
+                                  double mu, double barrier, int inverse,
+                                  hm_arith arith, void *stream);
+
 /* ---- measurement ------------------------------------------------------- */
 
 /* Times every tracking kernel launch with CUDA events on its stream while
