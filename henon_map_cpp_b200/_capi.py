@@ -97,7 +97,67 @@ _SIGNATURES = {
     "hm_fp64_peak": (None, [c_double, _PD, _PD]),
     "hm_set_profiling": (None, [c_int]),
     "hm_get_profile": (None, [_PD, POINTER(c_uint64)]),
+    # tangent map
+    "hm_matrices_create": (None, [c_size_t, POINTER(c_void_p)]),
+    "hm_matrices_destroy": (None, [c_void_p]),
+    "hm_matrices_size": (None, [c_void_p, POINTER(c_size_t)]),
+    "hm_matrices_reset": (None, [c_void_p]),
+    "hm_matrices_structured_multiply": (None, [c_void_p, c_void_p, c_void_p, c_double]),
+    "hm_matrices_set_with_tracker": (None, [c_void_p, c_void_p, c_void_p, c_double]),
+    "hm_matrices_copy": (None, [c_void_p, c_void_p]),
+    "hm_matrices_get": (None, [c_void_p, _PD]),
+    "hm_matrices_get_vector": (None, [c_void_p, _PD, _PD]),
+    "hm_vectors_create": (None, [_PD, c_size_t, POINTER(c_void_p)]),
+    "hm_vectors_destroy": (None, [c_void_p]),
+    "hm_vectors_set": (None, [c_void_p, _PD, c_int]),
+    "hm_vectors_multiply": (None, [c_void_p, c_void_p]),
+    "hm_vectors_normalize": (None, [c_void_p]),
+    "hm_vectors_get": (None, [c_void_p, _PD]),
+    # constructs
+    "hm_lyapunov_create": (None, [c_size_t, POINTER(c_uint64), c_size_t, POINTER(c_void_p)]),
+    "hm_lyapunov_destroy": (None, [c_void_p]),
+    "hm_lyapunov_reset": (None, [c_void_p]),
+    "hm_lyapunov_change_weights": (None, [c_void_p, c_uint64]),
+    "hm_lyapunov_add": (None, [c_void_p, c_void_p]),
+    "hm_lyapunov_windows": (None, [c_void_p, POINTER(c_size_t)]),
+    "hm_lyapunov_get_weights": (None, [c_void_p, c_size_t, _PD]),
+    "hm_lyapunov_get": (None, [c_void_p, c_int, _PD]),
+    "hm_megno_create": (None, [c_size_t, POINTER(c_void_p)]),
+    "hm_megno_destroy": (None, [c_void_p]),
+    "hm_megno_reset": (None, [c_void_p]),
+    "hm_megno_add": (None, [c_void_p, c_void_p, c_void_p]),
+    "hm_megno_get": (None, [c_void_p, _PD]),
+    "hm_megno_birkhoff_create": (None, [c_size_t, POINTER(c_uint64), c_size_t,
+                                        POINTER(c_void_p)]),
+    "hm_megno_birkhoff_destroy": (None, [c_void_p]),
+    "hm_megno_birkhoff_reset": (None, [c_void_p]),
+    "hm_megno_birkhoff_add": (None, [c_void_p, c_void_p, c_void_p]),
+    "hm_megno_birkhoff_get": (None, [c_void_p, _PD]),
+    "hm_tune_birkhoff_create": (None, [c_size_t, POINTER(c_uint64), c_size_t,
+                                       POINTER(c_void_p)]),
+    "hm_tune_birkhoff_destroy": (None, [c_void_p]),
+    "hm_tune_birkhoff_reset": (None, [c_void_p]),
+    "hm_tune_birkhoff_first_add": (None, [c_void_p, c_void_p]),
+    "hm_tune_birkhoff_add": (None, [c_void_p, c_void_p]),
+    "hm_tune_birkhoff_get": (None, [c_void_p, c_int, _PD]),
+    "hm_storage_create": (None, [c_size_t, c_size_t, POINTER(c_void_p)]),
+    "hm_storage_destroy": (None, [c_void_p]),
+    "hm_storage_store": (None, [c_void_p, c_void_p]),
+    "hm_storage_reset": (None, [c_void_p]),
+    "hm_storage_size": (None, [c_void_p, POINTER(c_size_t), POINTER(c_size_t),
+                               POINTER(c_size_t)]),
+    "hm_storage_get": (None, [c_void_p, c_int, _PD]),
+    "hm_storage_device_ptr": (None, [c_void_p, c_int, POINTER(c_void_p)]),
+    "hm_track_indicators": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, c_void_p]),
 }
+
+
+class IndicatorSet(ctypes.Structure):
+    """hm_indicator_set (include/henon_b200.h)."""
+    _fields_ = [("matrix", c_void_p), ("matrix_old", c_void_p), ("megno", c_void_p),
+                ("megno_birkhoff", c_void_p), ("vectors", c_void_p), ("lyapunov", c_void_p),
+                ("tune", c_void_p), ("megno_sample_turns", POINTER(c_uint64)),
+                ("n_megno_samples", c_size_t), ("megno_samples_out", _PD)]
 
 _lib: ctypes.CDLL | None = None
 
@@ -259,6 +319,231 @@ class Particles:
         if getattr(self, "h", None) and self.h.value and _lib is not None:
             _lib.hm_particles_destroy(self.h)
             self.h = c_void_p()
+
+
+class _Handle:
+    """Owns one opaque handle; `_destroy` names its hm_*_destroy."""
+
+    _destroy = ""
+
+    def __init__(self):
+        self.h = c_void_p()
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib is not None:
+            getattr(_lib, self._destroy)(self.h)
+            self.h = c_void_p()
+
+
+def _u64(values) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(values, dtype=np.uint64).ravel())
+
+
+class Matrices(_Handle):
+    """hm_matrices: one 4x4 matrix per particle (matrix_4d_vector_gpu)."""
+    _destroy = "hm_matrices_destroy"
+
+    def __init__(self, n: int):
+        super().__init__()
+        self.n = int(n)
+        call("hm_matrices_create", self.n, ctypes.byref(self.h))
+
+    def reset(self):
+        call("hm_matrices_reset", self.h)
+
+    def structured_multiply(self, tracker: Tracker, particles: Particles, mu: float):
+        call("hm_matrices_structured_multiply", self.h, tracker.h, particles.h, float(mu))
+
+    def set_with_tracker(self, tracker: Tracker, particles: Particles, mu: float):
+        call("hm_matrices_set_with_tracker", self.h, tracker.h, particles.h, float(mu))
+
+    def explicit_copy(self, other: "Matrices"):
+        call("hm_matrices_copy", self.h, other.h)
+
+    def get(self) -> np.ndarray:
+        out = np.empty((self.n, 4, 4))
+        call("hm_matrices_get", self.h, dptr(out))
+        return out
+
+    def get_vector(self, rv) -> np.ndarray:
+        rv = f64(rv).reshape(self.n, 4)
+        out = np.empty((self.n, 4))
+        call("hm_matrices_get_vector", self.h, dptr(rv), dptr(out))
+        return out
+
+
+class Vectors(_Handle):
+    """hm_vectors: one 4-vector per particle (vector_4d_gpu)."""
+    _destroy = "hm_vectors_destroy"
+
+    def __init__(self, rv):
+        super().__init__()
+        rv = f64(rv).reshape(-1, 4)
+        self.n = rv.shape[0]
+        call("hm_vectors_create", dptr(rv), self.n, ctypes.byref(self.h))
+
+    def set_vectors(self, rv):
+        rv = f64(rv)
+        if rv.size == 4 and self.n != 1:
+            call("hm_vectors_set", self.h, dptr(rv), 1)
+        else:
+            call("hm_vectors_set", self.h, dptr(rv.reshape(self.n, 4)), 0)
+
+    def multiply(self, m: Matrices):
+        call("hm_vectors_multiply", self.h, m.h)
+
+    def normalize(self):
+        call("hm_vectors_normalize", self.h)
+
+    def get(self) -> np.ndarray:
+        out = np.empty((self.n, 4))
+        call("hm_vectors_get", self.h, dptr(out))
+        return out
+
+
+class Lyapunov(_Handle):
+    """hm_lyapunov: lyapunov_birkhoff_construct(_multi)."""
+    _destroy = "hm_lyapunov_destroy"
+
+    def __init__(self, n: int, n_weights):
+        super().__init__()
+        self.n = int(n)
+        w = _u64(np.atleast_1d(n_weights))
+        self.lengths = [int(v) for v in w]
+        self.n_windows = w.size
+        call("hm_lyapunov_create", self.n, w.ctypes.data_as(POINTER(c_uint64)), w.size,
+             ctypes.byref(self.h))
+
+    def reset(self):
+        call("hm_lyapunov_reset", self.h)
+
+    def change_weights(self, n_weights: int):
+        call("hm_lyapunov_change_weights", self.h, int(n_weights))
+        self.lengths = [int(n_weights)]
+
+    def add(self, v: Vectors):
+        call("hm_lyapunov_add", self.h, v.h)
+
+    def weights(self, window: int = 0) -> np.ndarray:
+        out = np.empty(self.lengths[window])
+        call("hm_lyapunov_get_weights", self.h, int(window), dptr(out))
+        return out
+
+    def get(self, birkhoff: bool) -> np.ndarray:
+        out = np.empty((self.n_windows, self.n))
+        call("hm_lyapunov_get", self.h, int(bool(birkhoff)), dptr(out))
+        return out
+
+
+class Megno(_Handle):
+    _destroy = "hm_megno_destroy"
+
+    def __init__(self, n: int):
+        super().__init__()
+        self.n = int(n)
+        call("hm_megno_create", self.n, ctypes.byref(self.h))
+
+    def reset(self):
+        call("hm_megno_reset", self.h)
+
+    def add(self, a: Matrices, b: Matrices):
+        call("hm_megno_add", self.h, a.h, b.h)
+
+    def get(self) -> np.ndarray:
+        out = np.empty(self.n)
+        call("hm_megno_get", self.h, dptr(out))
+        return out
+
+
+class MegnoBirkhoff(_Handle):
+    _destroy = "hm_megno_birkhoff_destroy"
+
+    def __init__(self, n: int, turn_samples):
+        super().__init__()
+        self.n = int(n)
+        t = _u64(turn_samples)
+        self.n_samples = t.size
+        call("hm_megno_birkhoff_create", self.n, t.ctypes.data_as(POINTER(c_uint64)), t.size,
+             ctypes.byref(self.h))
+
+    def reset(self):
+        call("hm_megno_birkhoff_reset", self.h)
+
+    def add(self, a: Matrices, b: Matrices):
+        call("hm_megno_birkhoff_add", self.h, a.h, b.h)
+
+    def get(self) -> np.ndarray:
+        out = np.empty((self.n_samples, self.n))
+        call("hm_megno_birkhoff_get", self.h, dptr(out))
+        return out
+
+
+class TuneBirkhoff(_Handle):
+    _destroy = "hm_tune_birkhoff_destroy"
+
+    def __init__(self, n: int, turn_samples):
+        super().__init__()
+        self.n = int(n)
+        t = _u64(turn_samples)
+        self.n_samples = t.size
+        call("hm_tune_birkhoff_create", self.n, t.ctypes.data_as(POINTER(c_uint64)), t.size,
+             ctypes.byref(self.h))
+
+    def reset(self):
+        call("hm_tune_birkhoff_reset", self.h)
+
+    def first_add(self, p: Particles):
+        call("hm_tune_birkhoff_first_add", self.h, p.h)
+
+    def add(self, p: Particles):
+        call("hm_tune_birkhoff_add", self.h, p.h)
+
+    def get(self, which: int) -> np.ndarray:
+        out = np.empty((self.n_samples, self.n))
+        call("hm_tune_birkhoff_get", self.h, int(which), dptr(out))
+        return out
+
+
+class Storage(_Handle):
+    _destroy = "hm_storage_destroy"
+
+    def __init__(self, n: int, batch: int):
+        super().__init__()
+        self.n, self.batch = int(n), int(batch)
+        call("hm_storage_create", self.n, self.batch, ctypes.byref(self.h))
+
+    def store(self, p: Particles):
+        call("hm_storage_store", self.h, p.h)
+
+    def reset(self):
+        call("hm_storage_reset", self.h)
+
+    def get(self, field: int) -> np.ndarray:
+        out = np.empty((self.batch, self.n))
+        call("hm_storage_get", self.h, int(field), dptr(out))
+        return out
+
+
+def track_indicators(tracker: Tracker, particles: Particles, n_turns: int, mu: float,
+                     barrier: float = 100.0, matrix=None, matrix_old=None, megno=None,
+                     megno_birkhoff=None, vectors=None, lyapunov=None, tune=None,
+                     megno_sample_turns=None, megno_samples_out=None):
+    """hm_track_indicators: n_turns of the fused per-turn indicator loop."""
+    s = IndicatorSet()
+    for name, obj in (("matrix", matrix), ("matrix_old", matrix_old), ("megno", megno),
+                      ("megno_birkhoff", megno_birkhoff), ("vectors", vectors),
+                      ("lyapunov", lyapunov), ("tune", tune)):
+        setattr(s, name, obj.h.value if obj is not None else None)
+    keep = None
+    if megno_sample_turns is not None:
+        keep = _u64(megno_sample_turns)
+        s.megno_sample_turns = keep.ctypes.data_as(POINTER(c_uint64))
+        s.n_megno_samples = keep.size
+        if megno_samples_out is not None:
+            s.megno_samples_out = dptr(megno_samples_out)
+    call("hm_track_indicators", tracker.h, particles.h, int(n_turns), float(mu), float(barrier),
+         ctypes.byref(s))
+    del keep
 
 
 def set_track_config(threads: int, per_thread: int, chunk0: int, chunk_max: int) -> None:

@@ -24,15 +24,19 @@ LIB = PKG / "libhenon_b200.so"
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+# --fmad=false: no implicit contraction of a*b+c anywhere in device code.
+# The kernels spell their arithmetic explicitly (__d*_rn for the exact
+# path, fma() for the fast one); the flag makes CUDA's own libm (log, log10,
+# atan2) compile exactly as in the reference's --fmad=false build.
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--fmad=false",
               "-Xptxas", "-O3", *ARCH, f"-I{INCLUDE}"]
 # Host code: no -march and no contraction, so host doubles are plain SSE2
 # binary64 arithmetic like the reference's host build.
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
              f"-I{CUDA_HOME / 'include'}", f"-I{INCLUDE}"]
 
-CU_SOURCES = ["track.cu", "noalloc.cu"]
-CPP_SOURCES = ["capi.cpp", "modulation.cpp"]
+CU_SOURCES = ["track.cu", "noalloc.cu", "tangent.cu", "fused.cu"]
+CPP_SOURCES = ["capi.cpp", "modulation.cpp", "indicators.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

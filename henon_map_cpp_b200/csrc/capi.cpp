@@ -11,35 +11,6 @@
 
 #include "hm_internal.h"
 
-// ---- handles ------------------------------------------------------------------
-
-// Particle ensemble on the device (particles_4d_gpu, src/henon.h:119-193).
-struct hm_particles {
-    size_t n_total = 0;      // base particles + ghosts
-    size_t n_particles = 0;  // base particles
-    size_t n_ghosts = 0;     // ghosts per base particle
-    uint32_t global_steps = 0;
-    // steps value shared by every live (non-NaN) particle: all particles
-    // start at 0, survivors advance together and lost ones are frozen as NaN,
-    // so the table index of a whole track() call is uniform.
-    uint32_t live_step = 0;
-    // Host copies of what the reference keeps on the host side.
-    std::vector<double> x0, px0, y0, py0;
-    std::vector<uint8_t> valid, ghost;
-    std::vector<uint64_t> idx, idx_base;
-    hm::DeviceBuffer x, px, y, py, steps, dvalid, dghost, didx, didx_base;
-    hm::DeviceBuffer work;  // survivor lists of the chunked tracker
-    uint64_t rng_state = 0x9e3779b97f4a7c15ULL;
-};
-
-// Modulation tables on the device (henon_tracker_gpu, src/henon.h:212-228).
-struct hm_tracker {
-    uint64_t allowed_steps = 0;
-    std::vector<double> sx, cx, sy, cy;  // host copies
-    hm::DeviceBuffer table;              // {sx, cx, sy, cy} per turn
-    hm_arith arith = HM_ARITH_EXACT;
-};
-
 namespace hm {
 
 // ---- errors ---------------------------------------------------------------------

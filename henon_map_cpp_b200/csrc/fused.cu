@@ -1,0 +1,336 @@
+// Fused multi-turn tracking + tangent map + indicators (sm_100a).
+//
+// The reference computes indicators from Python, one turn at a time, with
+// 3-6 launches per turn (tests/test_construct.ipynb, test_new_standard.ipynb):
+//
+//     M_old.explicit_copy(M)                  (when MEGNO is accumulated)
+//     tracker.track(p, 1, mu, barrier)
+//     M.structured_multiply(tracker, p, mu)   DF(x_{n+1}; table[global_steps])
+//     megno.add(M, M_old); megno_b.add(M, M_old)
+//     J.set_with_tracker(tracker, p, mu); v.multiply(J); lyap.add(v); v.normalize()
+//     tune.add(p)
+//
+// This kernel runs that loop for a chunk of turns in one launch, one
+// particle per thread, with the orbit, M, v and the MEGNO layers in
+// registers and the per-window accumulators in shared memory.  Every step
+// uses the same separately rounded arithmetic and the same CUDA libm calls
+// as the per-call kernels (tangent.cu), so the results are bit-identical to
+// running the loop with the per-call API or with the reference CUDA build
+// compiled with --fmad=false.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hm_device.cuh"
+#include "hm_internal.h"
+
+namespace hm {
+namespace {
+
+using dev::Rn;
+
+__device__ __forceinline__ bool inside(double r, long long b2bits) {
+    return static_cast<unsigned long long>(__double_as_longlong(r)) <
+           static_cast<unsigned long long>(b2bits);
+}
+
+// One forward turn in the reference order (henon_step, src/henon.cu:482-542).
+template <bool OCT>
+__device__ __forceinline__ double map_turn(double &x, double &px, double &y, double &py,
+                                           const dev::Turn &t, double mu) {
+    const double xx = Rn::mul(x, x), yy = Rn::mul(y, y);
+    double npx = Rn::add(px, Rn::sub(xx, yy));
+    double npy = Rn::add(py, Rn::mul(Rn::mul(-2.0, x), y));
+    if (OCT) {
+        npx = Rn::add(npx, Rn::mul(mu, Rn::sub(Rn::mul(xx, x),
+                                               Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
+        npy = Rn::add(npy, Rn::mul(mu, Rn::sub(Rn::mul(yy, y),
+                                               Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
+    }
+    const double nx = Rn::add(Rn::mul(x, t.cx), Rn::mul(npx, t.sx));
+    npx = Rn::add(Rn::mul(-x, t.sx), Rn::mul(npx, t.cx));
+    const double ny = Rn::add(Rn::mul(y, t.cy), Rn::mul(npy, t.sy));
+    npy = Rn::add(Rn::mul(-y, t.sy), Rn::mul(npy, t.cy));
+    x = nx;
+    px = npx;
+    y = ny;
+    py = npy;
+    return Rn::add(Rn::add(Rn::mul(x, x), Rn::mul(px, px)), Rn::add(Rn::mul(y, y), Rn::mul(py, py)));
+}
+
+template <bool OCT, bool DO_M, bool DO_V, bool DO_T>
+__global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
+    extern __shared__ double smem[];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in_range = i < a.n;
+    const uint32_t ii = in_range ? i : 0;
+    // Per-thread window accumulators in shared memory, laid out [slot][thread]
+    // so that a warp touches 32 consecutive doubles.
+    const int T = blockDim.x;
+    double *mb_l2 = smem;                                  // [n_mb][T]
+    double *ly_raw = mb_l2 + size_t(a.n_mb) * T;           // [n_ly][T]
+    double *ly_b = ly_raw + size_t(a.n_ly) * T;            // [n_ly][T]
+    double *t1x = ly_b + size_t(a.n_ly) * T;               // [n_tu][T]
+    double *t1y = t1x + size_t(a.n_tu) * T;
+    double *t2x = t1y + size_t(a.n_tu) * T;
+    double *t2y = t2x + size_t(a.n_tu) * T;
+    const int tid = threadIdx.x;
+    const size_t n = a.n;
+
+    // ---- load state ---------------------------------------------------------
+    double x = a.x[ii], px = a.px[ii], y = a.y[ii], py = a.py[ii];
+    uint32_t steps = a.steps[ii];
+    bool alive = in_range && !dev::is_lost(x, px, y, py);
+    double M[16];
+    double old_norm = 0.0, m_l1 = 0.0, m_l2 = 0.0, m_l3 = 0.0, b_l1 = 0.0;
+    if (DO_M) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) M[k] = a.M[size_t(ii) * 16 + k];
+        old_norm = dev::norm_exact<16>(M);
+        if (a.megno_l1) {
+            m_l1 = a.megno_l1[ii];
+            m_l2 = a.megno_l2[ii];
+            m_l3 = a.megno_l3[ii];
+        }
+        if (a.mb_l1) b_l1 = a.mb_l1[ii];
+        for (int w = 0; w < a.n_mb; ++w) mb_l2[w * T + tid] = a.mb_l2[w * n + ii];
+    }
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (DO_V) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = a.V[size_t(ii) * 4 + k];
+        for (int w = 0; w < a.n_ly; ++w) {
+            ly_raw[w * T + tid] = a.ly_raw[w * n + ii];
+            ly_b[w * T + tid] = a.ly_b[w * n + ii];
+        }
+    }
+    double store_x = 0.0, store_y = 0.0;
+    if (DO_T) {
+        store_x = a.store_x[ii];
+        store_y = a.store_y[ii];
+        for (int w = 0; w < a.n_tu; ++w) {
+            t1x[w * T + tid] = a.t1x[w * n + ii];
+            t1y[w * T + tid] = a.t1y[w * n + ii];
+            t2x[w * T + tid] = a.t2x[w * n + ii];
+            t2y[w * T + tid] = a.t2y[w * n + ii];
+        }
+    }
+
+    const double mu = a.mu;
+    bool warp_live = __any_sync(dev::kFullMask, alive);
+    uint32_t k = 0;
+    for (; k < a.n_turns && warp_live; ++k) {
+        // ---- track(p, 1) ------------------------------------------------------
+        if (alive) {
+            const dev::Turn t = dev::load_turn(a.table, a.live_step + k);
+            const double r = map_turn<OCT>(x, px, y, py, t, mu);
+            if (inside(r, a.b2bits)) {
+                steps += 1u;
+            } else {
+                x = px = y = py = dev::quiet_nan();
+                alive = false;
+            }
+        }
+        // ---- tangent matrix at the new point, table[global_steps] -------------
+        double df[16];
+        if (DO_M || DO_V) {
+            const dev::Turn td = dev::load_turn(a.table, a.global_step + k + 1u);
+            dev::tangent_matrix_exact(x, y, td, mu, df);
+        }
+        if (DO_M) {
+            double out[16];
+            dev::matmul4_exact(df, M, out);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) M[q] = out[q];
+            const double new_norm = dev::norm_exact<16>(M);
+            const double lr = log10(Rn::div(new_norm, old_norm));
+            if (a.megno_l1) {
+                const double di = double(a.megno_idx + k);
+                m_l1 = Rn::add(m_l1, Rn::mul(lr, di));
+                m_l2 = Rn::add(m_l2, Rn::mul(Rn::div(1.0, di), m_l1));
+                m_l3 = Rn::mul(Rn::div(1.0, di), m_l2);
+                for (int j = 0; j < a.n_snap; ++j)
+                    if (a.snap_turns[j] == a.megno_idx + k && in_range)
+                        a.snap[size_t(j) * n + ii] = m_l3;
+            }
+            if (a.mb_l1) {
+                const uint64_t idx = a.mb_idx + k;
+                const double di = double(idx);
+                b_l1 = Rn::add(b_l1, Rn::mul(lr, di));
+                for (int w = 0; w < a.n_mb; ++w)
+                    if (idx <= a.mb_T[w]) {
+                        double &acc = mb_l2[w * T + tid];
+                        acc = Rn::add(acc, Rn::div(Rn::mul(b_l1, a.mb_w[a.mb_off[w] + idx - 1]), di));
+                    }
+            }
+            old_norm = new_norm;
+        }
+        if (DO_V) {
+            double t4[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                double s = 0.0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) s = Rn::add(s, Rn::mul(df[r * 4 + c], v[c]));
+                t4[r] = s;
+            }
+            const double nv = dev::norm_exact<4>(t4);
+            if (a.n_ly) {
+                const double l = log(nv);
+                const uint64_t idx = a.ly_idx + k;
+                for (int w = 0; w < a.n_ly; ++w) {
+                    const uint64_t len = a.ly_len[w];
+                    if (idx < len) {
+                        ly_raw[w * T + tid] = Rn::add(ly_raw[w * T + tid], Rn::div(l, double(len)));
+                        ly_b[w * T + tid] =
+                            Rn::add(ly_b[w * T + tid], Rn::mul(l, a.ly_w[a.ly_off[w] + idx]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[q] = Rn::div(t4[q], nv);
+        }
+        if (DO_T) {
+            const double ax = atan2(px, x), ay = atan2(py, y);
+            double dx = Rn::sub(ax, store_x), dy = Rn::sub(ay, store_y);
+            const double two_pi = 2 * M_PI;
+            dx = dx > 0 ? dx : Rn::add(dx, two_pi);
+            dy = dy > 0 ? dy : Rn::add(dy, two_pi);
+            store_x = ax;
+            store_y = ay;
+            const uint64_t idx = a.tu_idx + k;
+            for (int w = 0; w < a.n_tu; ++w) {
+                const uint64_t len = a.tu_T[w];
+                if (idx < len) {
+                    const double wt = a.tu_w[a.tu_off[w] + idx];
+                    t1x[w * T + tid] = Rn::add(t1x[w * T + tid], Rn::mul(dx, wt));
+                    t1y[w * T + tid] = Rn::add(t1y[w * T + tid], Rn::mul(dy, wt));
+                } else if (idx < 2 * len) {
+                    const double wt = a.tu_w[a.tu_off[w] + idx - len];
+                    t2x[w * T + tid] = Rn::add(t2x[w * T + tid], Rn::mul(dx, wt));
+                    t2y[w * T + tid] = Rn::add(t2y[w * T + tid], Rn::mul(dy, wt));
+                }
+            }
+        }
+        // A warp whose particles are all lost stops: every later update
+        // would only add NaN to windows that are still open (fixed below).
+        if (!alive) warp_live = __any_sync(dev::kFullMask, alive);
+    }
+
+    // ---- windows a stopped warp would still have touched become NaN --------
+    if (k < a.n_turns) {
+        const double nan = dev::quiet_nan();
+        const uint64_t left = a.n_turns - k;  // turns skipped
+        if (DO_M && a.megno_l1)
+            for (int j = 0; j < a.n_snap; ++j) {
+                const uint64_t s = a.snap_turns[j];
+                if (s >= a.megno_idx + k && s < a.megno_idx + a.n_turns && in_range)
+                    a.snap[size_t(j) * n + ii] = nan;
+            }
+        if (DO_M && a.mb_l1) {
+            const uint64_t idx = a.mb_idx + k;
+            for (int w = 0; w < a.n_mb; ++w)
+                if (idx <= a.mb_T[w]) mb_l2[w * T + tid] = nan;
+        }
+        if (DO_V) {
+            const uint64_t idx = a.ly_idx + k;
+            for (int w = 0; w < a.n_ly; ++w)
+                if (idx < a.ly_len[w]) {
+                    ly_raw[w * T + tid] = nan;
+                    ly_b[w * T + tid] = nan;
+                }
+        }
+        if (DO_T) {
+            const uint64_t first = a.tu_idx + k, last = a.tu_idx + k + left - 1;
+            for (int w = 0; w < a.n_tu; ++w) {
+                const uint64_t len = a.tu_T[w];
+                if (first < len) {
+                    t1x[w * T + tid] = nan;
+                    t1y[w * T + tid] = nan;
+                }
+                // window 2 is [len, 2 len): touched if it meets [first, last]
+                if (first < 2 * len && last >= len) {
+                    t2x[w * T + tid] = nan;
+                    t2y[w * T + tid] = nan;
+                }
+            }
+        }
+    }
+
+    if (!in_range) return;
+    // ---- store state --------------------------------------------------------
+    a.x[i] = x;
+    a.px[i] = px;
+    a.y[i] = y;
+    a.py[i] = py;
+    a.steps[i] = steps;
+    if (DO_M) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) a.M[size_t(i) * 16 + q] = M[q];
+        if (a.megno_l1) {
+            a.megno_l1[i] = m_l1;
+            a.megno_l2[i] = m_l2;
+            a.megno_l3[i] = m_l3;
+        }
+        if (a.mb_l1) a.mb_l1[i] = b_l1;
+        for (int w = 0; w < a.n_mb; ++w) a.mb_l2[w * n + i] = mb_l2[w * T + tid];
+    }
+    if (DO_V) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a.V[size_t(i) * 4 + q] = v[q];
+        for (int w = 0; w < a.n_ly; ++w) {
+            a.ly_raw[w * n + i] = ly_raw[w * T + tid];
+            a.ly_b[w * n + i] = ly_b[w * T + tid];
+        }
+    }
+    if (DO_T) {
+        a.store_x[i] = store_x;
+        a.store_y[i] = store_y;
+        for (int w = 0; w < a.n_tu; ++w) {
+            a.t1x[w * n + i] = t1x[w * T + tid];
+            a.t1y[w * n + i] = t1y[w * T + tid];
+            a.t2x[w * n + i] = t2x[w * T + tid];
+            a.t2y[w * n + i] = t2y[w * T + tid];
+        }
+    }
+}
+
+template <bool OCT, bool DO_M, bool DO_V, bool DO_T>
+cudaError_t launch4(const FusedArgs &a, cudaStream_t s) {
+    constexpr int threads = 128;
+    const size_t slots = size_t(a.n_mb) + 2 * size_t(a.n_ly) + 4 * size_t(a.n_tu);
+    const size_t smem = slots * threads * sizeof(double);
+    auto k = indicators_kernel<OCT, DO_M, DO_V, DO_T>;
+    if (smem > 48 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    const unsigned blocks = unsigned((a.n + threads - 1) / threads);
+    k<<<blocks, threads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool OCT>
+cudaError_t launch_oct(const FusedArgs &a, cudaStream_t s) {
+    const bool m = a.M != nullptr, v = a.V != nullptr, t = a.store_x != nullptr;
+    if (m && v && t) return launch4<OCT, true, true, true>(a, s);
+    if (m && v) return launch4<OCT, true, true, false>(a, s);
+    if (m && t) return launch4<OCT, true, false, true>(a, s);
+    if (v && t) return launch4<OCT, false, true, true>(a, s);
+    if (m) return launch4<OCT, true, false, false>(a, s);
+    if (v) return launch4<OCT, false, true, false>(a, s);
+    if (t) return launch4<OCT, false, false, true>(a, s);
+    return launch4<OCT, false, false, false>(a, s);
+}
+
+}  // namespace
+
+size_t fused_max_slots() { return 96; }
+
+cudaError_t launch_indicators(const FusedArgs &a, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    return a.mu != 0.0 ? launch_oct<true>(a, s) : launch_oct<false>(a, s);
+}
+
+}  // namespace hm

@@ -65,6 +65,39 @@ struct DeviceBuffer {
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+}  // namespace hm
+
+// ---- handles ------------------------------------------------------------------
+
+// Particle ensemble on the device (particles_4d_gpu, src/henon.h:119-193).
+struct hm_particles {
+    size_t n_total = 0;      // base particles + ghosts
+    size_t n_particles = 0;  // base particles
+    size_t n_ghosts = 0;     // ghosts per base particle
+    uint32_t global_steps = 0;
+    // steps value shared by every live (non-NaN) particle: all particles
+    // start at 0, survivors advance together and lost ones are frozen as NaN,
+    // so the table index of a whole track() call is uniform.
+    uint32_t live_step = 0;
+    // Host copies of what the reference keeps on the host side.
+    std::vector<double> x0, px0, y0, py0;
+    std::vector<uint8_t> valid, ghost;
+    std::vector<uint64_t> idx, idx_base;
+    hm::DeviceBuffer x, px, y, py, steps, dvalid, dghost, didx, didx_base;
+    hm::DeviceBuffer work;  // survivor lists of the chunked tracker
+    uint64_t rng_state = 0x9e3779b97f4a7c15ULL;
+};
+
+// Modulation tables on the device (henon_tracker_gpu, src/henon.h:212-228).
+struct hm_tracker {
+    uint64_t allowed_steps = 0;
+    std::vector<double> sx, cx, sy, cy;  // host copies
+    hm::DeviceBuffer table;              // {sx, cx, sy, cy} per turn
+    hm_arith arith = HM_ARITH_EXACT;
+};
+
+namespace hm {
+
 // ---- kernel launchers (defined in the .cu files) ---------------------------
 
 // Parameters of one fused multi-turn chunk launch over a list of particles.
@@ -130,5 +163,85 @@ cudaError_t launch_observable(const double *x, const double *px,
 // FP64 FMA-chain microbenchmark launcher; returns flops per launch.
 cudaError_t launch_fp64_peak(double *sink, int blocks, int threads,
                              int iters, cudaStream_t s, double *flops);
+
+// Tangent-map and indicator kernels (tangent.cu).
+cudaError_t launch_matrices_step(double *M, const double *x, const double *px, const double *y,
+                                 const double *py, const double *table, uint32_t idx, double mu,
+                                 size_t n, bool set, cudaStream_t s);
+cudaError_t launch_matrices_identity(double *M, size_t n, cudaStream_t s);
+cudaError_t launch_matrices_apply(const double *M, const double *rv, double *out, size_t n,
+                                  cudaStream_t s);
+cudaError_t launch_vectors_multiply(const double *M, double *V, size_t n, cudaStream_t s);
+cudaError_t launch_vectors_normalize(double *V, size_t n, cudaStream_t s);
+cudaError_t launch_lyapunov(double *raw, double *bsum, const double *V, const double *weights,
+                            const uint64_t *w_off, const uint64_t *w_len, int n_windows,
+                            size_t idx, size_t n, cudaStream_t s);
+cudaError_t launch_megno(double *l1, double *l2, double *l3, const double *A, const double *B,
+                         size_t idx, size_t n, cudaStream_t s);
+cudaError_t launch_megno_birkhoff(double *l1, double *l2, const double *weights,
+                                  const uint64_t *w_off, const uint64_t *T, int n_windows,
+                                  const double *A, const double *B, size_t idx, size_t n,
+                                  cudaStream_t s);
+cudaError_t launch_tune_init(const double *x, const double *px, const double *y, const double *py,
+                             double *store_x, double *store_y, size_t n, cudaStream_t s);
+cudaError_t launch_tune_add(const double *x, const double *px, const double *y, const double *py,
+                            double *store_x, double *store_y, double *t1x, double *t1y,
+                            double *t2x, double *t2y, const double *weights,
+                            const uint64_t *w_off, const uint64_t *T, int n_windows, size_t idx,
+                            size_t n, cudaStream_t s);
+
+// Arguments of the fused tracking + indicator kernel (fused.cu).  Null
+// pointers switch parts off: M (tangent matrix, MEGNO), V (tangent vectors,
+// Lyapunov), store_x (Birkhoff tunes).  Window tables are on the device.
+struct FusedArgs {
+    double *x, *px, *y, *py;
+    uint32_t *steps;
+    uint32_t n;
+    const double *table;
+    uint32_t live_step;    // table index of the map for the first turn
+    uint32_t global_step;  // global_steps before the first turn
+    uint32_t n_turns;
+    double mu;
+    long long b2bits;
+    // tangent matrix and MEGNO
+    double *M;
+    double *megno_l1, *megno_l2, *megno_l3;
+    uint64_t megno_idx;
+    double *snap;
+    const uint64_t *snap_turns;
+    int n_snap;
+    double *mb_l1, *mb_l2;
+    uint64_t mb_idx;
+    const uint64_t *mb_T, *mb_off;
+    const double *mb_w;
+    int n_mb;
+    // tangent vectors and Lyapunov windows
+    double *V;
+    double *ly_raw, *ly_b;
+    uint64_t ly_idx;
+    const uint64_t *ly_len, *ly_off;
+    const double *ly_w;
+    int n_ly;
+    // Birkhoff tunes
+    double *store_x, *store_y, *t1x, *t1y, *t2x, *t2y;
+    uint64_t tu_idx;
+    const uint64_t *tu_T, *tu_off;
+    const double *tu_w;
+    int n_tu;
+};
+
+cudaError_t launch_indicators(const FusedArgs &a, cudaStream_t s);
+// Largest number of per-thread window accumulators the fused kernel takes
+// (n_megno_birkhoff + 2 n_lyapunov + 4 n_tune).
+size_t fused_max_slots();
+
+// Uploads a host vector to a fresh device buffer.
+template <class T>
+hm_status upload(DeviceBuffer &dst, const std::vector<T> &src) {
+    HM_TRY(dst.alloc(src.size() * sizeof(T)));
+    if (!src.empty())
+        HM_CUDA_TRY(cudaMemcpy(dst.ptr, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return ok();
+}
 
 }  // namespace hm

@@ -190,6 +190,152 @@ hm_status hm_track_device(double *x, double *px, double *y, double *py,
                           int inverse, hm_arith arith, void *workspace,
                           void *stream);
 
+/* ---- tangent map (matrix_4d_vector_gpu, vector_4d_gpu) ------------------
+ * One 4x4 matrix / 4-vector per particle on the device.  Each call is one
+ * elementwise launch with the reference's arithmetic order, so results are
+ * bit-identical to the reference CUDA build with --fmad=false. */
+
+typedef struct hm_matrices hm_matrices;
+typedef struct hm_vectors hm_vectors;
+
+/* matrix_4d_vector_gpu(N): N identity matrices (src/henon.cu:1789-1808). */
+hm_status hm_matrices_create(size_t n, hm_matrices **out);
+hm_status hm_matrices_destroy(hm_matrices *m);
+hm_status hm_matrices_size(const hm_matrices *m, size_t *n);
+/* Back to identity (the reference's reset is a no-op, src/henon.cu:1815). */
+hm_status hm_matrices_reset(hm_matrices *m);
+/* M <- DF(x; table[global_steps]) * M (structured_multiply, :1827-1835). */
+hm_status hm_matrices_structured_multiply(hm_matrices *m, const hm_tracker *t,
+                                          const hm_particles *p, double mu);
+/* M <- DF(x; table[global_steps]) (set_with_tracker, :1837-1845). */
+hm_status hm_matrices_set_with_tracker(hm_matrices *m, const hm_tracker *t,
+                                       const hm_particles *p, double mu);
+/* explicit_copy (:1907-1912). */
+hm_status hm_matrices_copy(hm_matrices *dst, const hm_matrices *src);
+/* Host copy, double[n][16] row-major (get_matrix, :1914-1946). */
+hm_status hm_matrices_get(const hm_matrices *m, double *host_out);
+/* out[i] = M[i] rv[i], double[n][4] (get_vector, :1847-1905). */
+hm_status hm_matrices_get_vector(const hm_matrices *m, const double *host_rv,
+                                 double *host_out);
+
+/* vector_4d_gpu(rv): double[n][4] (src/henon.cu:1948-1971). */
+hm_status hm_vectors_create(const double *host, size_t n, hm_vectors **out);
+hm_status hm_vectors_destroy(hm_vectors *v);
+/* set_vectors (:1978-2007): host double[n][4], or one 4-vector repeated
+ * when broadcast != 0. */
+hm_status hm_vectors_set(hm_vectors *v, const double *host, int broadcast);
+/* v <- M v (multiply, :2009-2013). */
+hm_status hm_vectors_multiply(hm_vectors *v, const hm_matrices *m);
+/* v <- v / |v| (normalize, :2015-2019). */
+hm_status hm_vectors_normalize(hm_vectors *v);
+hm_status hm_vectors_get(const hm_vectors *v, double *host_out);
+
+/* ---- indicator constructs ------------------------------------------------ */
+
+typedef struct hm_lyapunov hm_lyapunov;
+typedef struct hm_megno hm_megno;
+typedef struct hm_megno_birkhoff hm_megno_birkhoff;
+typedef struct hm_tune_birkhoff hm_tune_birkhoff;
+typedef struct hm_storage hm_storage;
+
+/* lyapunov_birkhoff_construct (one window, src/henon.cu:2042-2128) and
+ * lyapunov_birkhoff_construct_multi (src/henon.cu:2130-2220): per add, for
+ * every window w with idx < n_w: raw_w += log|v|/n_w, b_w += log|v| w[idx].
+ * (The reference's one-window add has no idx < n_w guard, :2103; here it
+ * has.) */
+hm_status hm_lyapunov_create(size_t n, const uint64_t *n_weights,
+                             size_t n_windows, hm_lyapunov **out);
+hm_status hm_lyapunov_destroy(hm_lyapunov *h);
+hm_status hm_lyapunov_reset(hm_lyapunov *h);
+hm_status hm_lyapunov_change_weights(hm_lyapunov *h, uint64_t n_weights);
+hm_status hm_lyapunov_add(hm_lyapunov *h, const hm_vectors *v);
+hm_status hm_lyapunov_windows(const hm_lyapunov *h, size_t *n_windows);
+hm_status hm_lyapunov_get_weights(const hm_lyapunov *h, size_t window,
+                                  double *host_out);
+/* birkhoff 0: get_values_raw, 1: get_values_b; double[n_windows][n]. */
+hm_status hm_lyapunov_get(const hm_lyapunov *h, int birkhoff,
+                          double *host_out);
+
+/* megno_construct (src/henon.cu:2223-2299): with a = |A|_F, b = |B|_F,
+ * L1 += log10(a/b)*idx, L2 += L1/idx, value = L2/idx (idx from 1). */
+hm_status hm_megno_create(size_t n, hm_megno **out);
+hm_status hm_megno_destroy(hm_megno *h);
+hm_status hm_megno_reset(hm_megno *h);
+hm_status hm_megno_add(hm_megno *h, const hm_matrices *a, const hm_matrices *b);
+hm_status hm_megno_get(const hm_megno *h, double *host_out);
+
+/* megno_birkhoff_construct (src/henon.cu:2302-2426): windows T_j,
+ * L2_j += L1 * w_Tj[idx-1] / idx while idx <= T_j; double[n_samples][n]. */
+hm_status hm_megno_birkhoff_create(size_t n, const uint64_t *turn_samples,
+                                   size_t n_samples, hm_megno_birkhoff **out);
+hm_status hm_megno_birkhoff_destroy(hm_megno_birkhoff *h);
+hm_status hm_megno_birkhoff_reset(hm_megno_birkhoff *h);
+hm_status hm_megno_birkhoff_add(hm_megno_birkhoff *h, const hm_matrices *a,
+                                const hm_matrices *b);
+hm_status hm_megno_birkhoff_get(const hm_megno_birkhoff *h, double *host_out);
+
+/* tune_birkhoff_construct (src/henon.cu:2428-2655): phase advance
+ * atan2(p, q) wrapped to (0, 2pi], weighted into [0, T) and [T, 2T).
+ * which: 0 tune1_x, 1 tune1_y, 2 tune2_x, 3 tune2_y; double[n_samples][n].
+ * Accumulators start at zero (the reference leaves them uninitialised
+ * until reset()). */
+hm_status hm_tune_birkhoff_create(size_t n, const uint64_t *turn_samples,
+                                  size_t n_samples, hm_tune_birkhoff **out);
+hm_status hm_tune_birkhoff_destroy(hm_tune_birkhoff *h);
+hm_status hm_tune_birkhoff_reset(hm_tune_birkhoff *h);
+hm_status hm_tune_birkhoff_first_add(hm_tune_birkhoff *h, const hm_particles *p);
+hm_status hm_tune_birkhoff_add(hm_tune_birkhoff *h, const hm_particles *p);
+hm_status hm_tune_birkhoff_get(const hm_tune_birkhoff *h, int which,
+                               double *host_out);
+
+/* storage_4d_gpu (src/henon.cu:3351-3462): batch snapshots of x, px, y, py;
+ * double[batch][n] per field.  store() past batch_size is refused (the
+ * reference writes past its buffers). */
+hm_status hm_storage_create(size_t n, size_t batch, hm_storage **out);
+hm_status hm_storage_destroy(hm_storage *h);
+hm_status hm_storage_store(hm_storage *h, const hm_particles *p);
+hm_status hm_storage_reset(hm_storage *h);
+hm_status hm_storage_size(const hm_storage *h, size_t *n, size_t *batch,
+                          size_t *stored);
+hm_status hm_storage_get(const hm_storage *h, hm_field field, double *host_out);
+hm_status hm_storage_device_ptr(const hm_storage *h, hm_field field,
+                                const double **out);
+
+/* ---- fused tracking + indicators ----------------------------------------
+ * hm_track_indicators runs n_turns iterations of the per-turn loop that the
+ * reference drives from Python (tests/test_construct.ipynb,
+ * tests/test_new_standard.ipynb), in chunked multi-turn launches:
+ *     matrix_old <- matrix                     (when given)
+ *     track(p, 1, mu, barrier)                 (hm_track)
+ *     matrix.structured_multiply(t, p, mu)     (when matrix)
+ *     megno.add(matrix, matrix_old)            (when megno)
+ *     megno_birkhoff.add(matrix, matrix_old)   (when megno_birkhoff)
+ *     J.set_with_tracker(t, p, mu); vectors.multiply(J);
+ *     lyapunov.add(vectors); vectors.normalize()  (when vectors)
+ *     tune.add(p)                              (when tune)
+ * Every handle ends in the state the loop leaves it in, bit for bit.  The
+ * MEGNO layer-3 value is also recorded into megno_samples_out[j][i] when
+ * megno's add counter equals megno_sample_turns[j].  All construct sizes
+ * must equal the particle count; the tracker needs global_steps + n_turns
+ * + 1 table entries when a tangent part is on (structured_multiply reads
+ * table[global_steps] after the turn). */
+typedef struct hm_indicator_set {
+    hm_matrices *matrix;
+    hm_matrices *matrix_old;
+    hm_megno *megno;
+    hm_megno_birkhoff *megno_birkhoff;
+    hm_vectors *vectors;
+    hm_lyapunov *lyapunov;
+    hm_tune_birkhoff *tune;
+    const uint64_t *megno_sample_turns;
+    size_t n_megno_samples;
+    double *megno_samples_out; /* host double[n_megno_samples][n] or NULL */
+} hm_indicator_set;
+
+hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns,
+                              double mu, double barrier,
+                              const hm_indicator_set *set);
+
 /* No counterpart in the reference.  The same operation as hm_track_device
  * for callers that cannot allocate device memory (an application that
  * reserves all device memory at start-up, a framework whose allocator owns

@@ -165,6 +165,45 @@ def reference_module(variant: str = "fmad_off"):
     return mod
 
 
+_CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from oracle import oracle as O
+d = np.load(sys.argv[3])
+R = O.reference_module(sys.argv[2])
+kind, cls_t, cls_p = (("gpu", R.henon_tracker_gpu, R.particles_4d_gpu) if int(d["gpu"])
+                      else ("cpu", R.henon_tracker, R.particles_4d))
+t = cls_t(int(d["n_turns"]), float(d["tunes"][0]), float(d["tunes"][1]), "sps", float("nan"),
+          float(d["epsilon"]), 0)
+p = cls_p(d["x"], d["px"], d["y"], d["py"])
+t.track(p, int(d["n_turns"]), float(d["mu"]), float(d["barrier"]))
+np.savez(sys.argv[4], x=np.asarray(p.get_x()), px=np.asarray(p.get_px()),
+         y=np.asarray(p.get_y()), py=np.asarray(p.get_py()), steps=np.asarray(p.get_steps()))
+"""
+
+
+def reference_track_subprocess(variant: str, x, px, y, py, n_turns: int, tunes, epsilon: float,
+                               mu: float, barrier: float = 10.0, gpu: bool = True):
+    """Tracks with the reference build `variant` in a child interpreter.
+
+    Two builds of the reference share one pybind11 module name, so only one
+    of them can live in a process; the child keeps them apart.  Returns
+    (x, px, y, py, steps) or None when the build is absent."""
+    import tempfile
+
+    if not (REF_DIR / variant).exists():
+        return None
+    with tempfile.TemporaryDirectory() as tmp:
+        inp, out = Path(tmp) / "in.npz", Path(tmp) / "out.npz"
+        np.savez(inp, x=np.asarray(x, float), px=np.asarray(px, float), y=np.asarray(y, float),
+                 py=np.asarray(py, float), n_turns=n_turns, tunes=np.asarray(tunes, float),
+                 epsilon=epsilon, mu=mu, barrier=barrier, gpu=int(gpu))
+        subprocess.run([sys.executable, "-c", _CHILD, str(HERE.parent), variant, str(inp),
+                        str(out)], check=True)
+        d = np.load(out)
+        return d["x"], d["px"], d["y"], d["py"], d["steps"].astype(np.uint32)
+
+
 def build_reference() -> bool:
     """Runs oracle/build_ref.sh when the reference sources are present."""
     if not Path(os.environ.get("REF", "/root/reference"), "src").exists():

@@ -67,6 +67,37 @@ def test_oracle_notebook_known_answers():
     np.testing.assert_allclose(np.log(np.linalg.norm(v)), vm["log_norm"], rtol=1e-12)
 
 
+def test_indicator_oracle_pinned():
+    from oracle import indicators as I
+
+    nb = golden_json("notebook_values.json")
+    sx, cx, sy, cy = O.tables(1001, *TUNES, "sps", epsilon=0.0)
+    m = I.tangent_matrix([0.1], [0.1], sx[0], cx[0], sy[0], cy[0], 0.0)[0]
+    np.testing.assert_allclose(m, nb["tangent_matrix_x0"]["matrix"], rtol=1e-7, atol=1e-8)
+    rng = np.random.default_rng(3)
+    for mu in (0.0, 0.3, -0.7):
+        xs, ys = rng.normal(size=5), rng.normal(size=5)
+        mats = I.tangent_matrix(xs, ys, sx[7], cx[7], sy[7], cy[7], mu)
+        for k in range(5):
+            c = O.tangent_matrix(xs[k], 0.0, ys[k], 0.0, sx[7], cx[7], sy[7], cy[7], mu)
+            assert_bitwise(mats[k], c)
+            assert_bitwise(I.matmul(mats[k:k + 1], mats[k:k + 1])[0], O.matmul4(c, c))
+    # Lyapunov windows of the notebook: v = (1, 1, 0, 0) every turn.
+    lw = nb["lyapunov_multi_windows"]
+    nv = I.norm(np.array([[1.0, 1.0, 0.0, 0.0]]))[0]
+    for tag, k in (("5", 5), ("10", 10), ("15", 15)):
+        raw = [sum(np.log(nv) / L for i in range(min(k, L))) for L in (5, 10, 15)]
+        bw = [sum(np.log(nv) * O.birkhoff_weights(L)[i] for i in range(min(k, L)))
+              for L in (5, 10, 15)]
+        np.testing.assert_allclose(raw, lw[f"raw_after_{tag}"], rtol=1e-7, atol=5e-9)
+        np.testing.assert_allclose(bw, lw[f"b_after_{tag}"], rtol=1e-7, atol=5e-9)
+    # The loop runs and loses the large-amplitude particles.
+    x, px, y, py = grid(0.6, 8)
+    L = I.ConstructLoop(x, px, y, py, (sx, cx, sy, cy), 0.0, 10.0, [1, 0, 0, 0], [10, 50],
+                        [10, 50], [20, 40]).run(100)
+    assert np.isnan(L.m_l3).any() and np.isfinite(L.m_l3).any()
+
+
 @pytest.mark.skipif(O.reference_module("fmad_off") is None, reason="reference build absent")
 @pytest.mark.parametrize("eps,mu,nt", [(0.0, 0.0, 1500), (16.0, 0.2, 1500), (64.0, -0.3, 1200)])
 def test_oracle_equals_reference_build_live(eps, mu, nt):

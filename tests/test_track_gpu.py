@@ -213,12 +213,9 @@ def test_fast_arith_tolerances(gpu):
     assert np.mean(surv_e == surv_f) >= 0.93, np.mean(surv_e == surv_f)
     # The reference's own CUDA path as shipped (FMA contraction) on the same
     # grid: our FAST mode must be as close to the exact result as it is.
-    R = O.reference_module("default")
-    if R is not None:
-        rt = R.henon_tracker_gpu(N, TUNES[0], TUNES[1], "sps", NAN, 64.0, 0)
-        rp = R.particles_4d_gpu(gx, gpx, gy, gpy)
-        rt.track(rp, N, 0.2, 10.0)
-        ref_steps = np.asarray(rp.get_steps())
+    ref = O.reference_track_subprocess("default", gx, gpx, gy, gpy, N, TUNES, 64.0, 0.2)
+    if ref is not None:
+        ref_steps = ref[4]
         ours_equal = np.mean(fast[4] == exact[4])
         ref_equal = np.mean(ref_steps == exact[4])
         ref_surv = np.mean((ref_steps == N).reshape(side, side) == surv_e)
