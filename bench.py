@@ -62,6 +62,8 @@ def parse_args():
     ap.add_argument("--arith", choices=["exact", "fast"], default="exact")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched / adjoint / indicator measurements")
     return ap.parse_args()
 
 
@@ -187,6 +189,151 @@ def reference_cpu_sample(turns: int, side: int, target_s: float = 20.0):
             "sample": f"every {stride}th grid point per axis ({n} particles) x {turns} turns x "
                       f"6 (eps, mu) scans = {nominal:.3g} nominal particle-turns in {dt:.2f} s "
                       f"(table setup included)"}
+
+
+# ---- supplementary measurements (one GPU) ---------------------------------------------
+
+def bench_batched(C, arith):
+    """Mixed-size workload: 64 parameter sets, log-uniform 1k-256k particles
+    in the 4D ball r < 0.6 and 1e3-1e6 turns, as one batch (graph replay)
+    versus one plain tracking call per set.  Survival counts must agree."""
+    import torch
+
+    from henon_map_cpp_b200 import sweep
+
+    sets, coords = sweep.heterogeneous_sets(seed=20261203)
+    b = C.Batch(sets)
+    b.configure(arith, 2, 512, 16384)
+    b.load(*coords)
+    b.run(True)  # capture + warm-up
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        b.run(True)
+        times.append(time.perf_counter() - t0)
+    t_batch = min(times)
+    steps_batch = b.get(C.FIELD_STEPS)
+    # plain: one chunked tracking call per set on device arrays
+    t_plain, equal, o = 0.0, True, 0
+    stream = torch.cuda.current_stream().cuda_stream
+    for s in sets:
+        n = s["n_particles"]
+        tr = C.Tracker(s["n_turns"], s["omega_x"], s["omega_y"], "sps", float("nan"),
+                       s["epsilon"], 0)
+        dev = [torch.from_numpy(np.ascontiguousarray(c[o:o + n])).cuda() for c in coords]
+        st = torch.zeros(n, dtype=torch.int32, device="cuda")
+        ws = torch.empty(C.load().hm_track_workspace_bytes(n), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        C.call("hm_track_device", *[d.data_ptr() for d in dev], st.data_ptr(), n,
+               tr.device_tables(), s["n_turns"], 0, s["n_turns"], s["mu"], s["barrier"], 0,
+               arith, ws.data_ptr(), stream)
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+        equal &= bool(np.array_equal(st.cpu().numpy().view(np.uint32), steps_batch[o:o + n]))
+        o += n
+    nominal = float(sum(s["n_particles"] * s["n_turns"] for s in sets))
+    return {"workload": "64 sets, tunes U[0.15,0.32], eps U[0,64], mu U[-0.5,0.5], "
+                        "log-uniform 1e3-2.56e5 particles in the 4D ball r<0.6, "
+                        "log-uniform 1e3-1e6 turns (seed 20261203)",
+            "particles": int(sum(s["n_particles"] for s in sets)),
+            "nominal_particle_turns": nominal, "executed_particle_turns": float(steps_batch.sum()),
+            "batched_s": t_batch, "plain_sum_s": t_plain, "speedup": t_plain / t_batch,
+            "batched_value": nominal / t_batch, "survival_equal_to_plain": equal,
+            "n_chunks": b.n_chunks(), "timing": "wall clock around synchronous runs, best of 2"}
+
+
+def bench_adjoint(C):
+    """Adjoint of the Birkhoff-weighted orbit loss: 65,536 particles,
+    x0, y0 ~ U[0, 0.3], px0, py0 ~ N(0, 0.01^2), eps 16, mu 0.1, 1e4 turns,
+    checkpoints every 100 turns; versus one forward tracking pass."""
+    import math
+
+    import torch
+
+    from henon_map_cpp_b200 import autograd as AG
+
+    rng = np.random.default_rng(5)
+    n, nt = 65_536, 10_000
+    pts = [torch.tensor(a, device="cuda") for a in
+           (rng.uniform(0, 0.3, n), rng.normal(0, 0.01, n), rng.uniform(0, 0.3, n),
+            rng.normal(0, 0.01, n))]
+    theta = torch.tensor([2 * math.pi * 0.168, 2 * math.pi * 0.201, 16.0, 0.1],
+                         dtype=torch.float64)
+
+    def timed(fn, reps=3):
+        fn()
+        best = 1e30
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            best = min(best, a.elapsed_time(b) * 1e-3)
+        return best
+
+    t_adj = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100))
+    t_loss = timed(lambda: AG.per_particle(*pts, theta, nt, mode="loss"))
+    tr = C.Tracker(nt, 0.168, 0.201, "sps", float("nan"), 16.0, 0)
+    work = [torch.empty_like(p) for p in pts]
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ws = torch.empty(C.load().hm_track_workspace_bytes(n), dtype=torch.uint8, device="cuda")
+
+    def track():
+        for w_, p in zip(work, pts):
+            w_.copy_(p)
+        st.zero_()
+        C.call("hm_track_device", *[w_.data_ptr() for w_ in work], st.data_ptr(), n,
+               tr.device_tables(), nt, 0, nt, 0.1, 10.0, 0, C.ARITH_EXACT, ws.data_ptr(),
+               torch.cuda.current_stream().cuda_stream)
+
+    t_track = timed(track)
+    r = AG.per_particle(*pts, theta, nt, checkpoint_every=100)
+    return {"workload": "65,536 particles, 1e4 turns, eps 16, mu 0.1, checkpoints every 100",
+            "adjoint_s": t_adj, "forward_track_s": t_track, "forward_loss_s": t_loss,
+            "adjoint_over_forward_track": t_adj / t_track,
+            "survivors": int(r["survived"].sum().item()),
+            "timing": "CUDA events, best of 3 after one warm-up"}
+
+
+def bench_indicators(C, turns=100_000):
+    """Tangent map + indicators fused: 512x512 grid on [0, 0.4]^2, eps 32,
+    mu 0, windows at the 13 log-spaced turns 1e2..1e5 (MEGNO, Birkhoff-MEGNO,
+    Lyapunov with tangent vectors, Birkhoff tunes)."""
+    import torch
+
+    side = 512
+    v = np.linspace(0.0, 0.4, side)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    z = np.zeros_like(x)
+    n = x.size
+    T = [int(t) for t in np.unique(np.round(np.logspace(2, 5, 13)))]
+
+    def run(nt):
+        tr = C.Tracker(nt + 1, 0.168, 0.201, "sps", float("nan"), 32.0, 0)
+        p = C.Particles(x, z, y, z)
+        objs = dict(matrix=C.Matrices(n), megno=C.Megno(n), megno_birkhoff=C.MegnoBirkhoff(n, T),
+                    vectors=C.Vectors(np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))),
+                    lyapunov=C.Lyapunov(n, T), tune=C.TuneBirkhoff(n, T))
+        objs["tune"].first_add(p)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        C.track_indicators(tr, p, nt, 0.0, 10.0, **objs)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, p
+
+    run(1000)
+    dt, p = run(turns)
+    steps = p.get(C.FIELD_STEPS)
+    return {"workload": f"512x512 grid on [0,0.4]^2, eps 32, mu 0, {turns} turns, "
+                        "MEGNO + Birkhoff-MEGNO + Lyapunov + Birkhoff tunes at 13 windows",
+            "seconds": dt, "nominal_particle_turns_per_s": n * turns / dt,
+            "executed_particle_turns_per_s": float(steps.sum()) / dt,
+            "timing": "wall clock around one synchronous call (4096-turn launches)"}
 
 
 # ---- reference arm ---------------------------------------------------------------
@@ -363,6 +510,12 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu_sample(args.turns, args.side)
 
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras["batched"] = bench_batched(C, arith)
+        extras["adjoint"] = bench_adjoint(C)
+        extras["indicators"] = bench_indicators(C)
+
     if rank == 0:
         peak_unit = "TFLOP/s"
         line = {
@@ -387,6 +540,7 @@ def run_ours(args):
             "clocks": clock_summary,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            **extras,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -149,7 +149,34 @@ _SIGNATURES = {
     "hm_storage_get": (None, [c_void_p, c_int, _PD]),
     "hm_storage_device_ptr": (None, [c_void_p, c_int, POINTER(c_void_p)]),
     "hm_track_indicators": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, c_void_p]),
+    # ghosts and host tangent matrices
+    "hm_particles_add_ghost": (None, [c_void_p, c_double, c_char_p]),
+    "hm_particles_renormalize": (None, [c_void_p, c_double]),
+    "hm_particles_displacement_module": (None, [c_void_p, _PD]),
+    "hm_particles_displacement_direction": (None, [c_void_p, _PD]),
+    "hm_tracker_tangent_matrices": (None, [c_void_p, c_void_p, c_double, c_int, _PD]),
+    # batched heterogeneous tracking
+    "hm_batch_create": (None, [c_size_t, c_void_p, POINTER(c_void_p)]),
+    "hm_batch_destroy": (None, [c_void_p]),
+    "hm_batch_configure": (None, [c_void_p, c_int, c_int, c_uint32, c_uint32]),
+    "hm_batch_size": (None, [c_void_p, POINTER(c_uint64), POINTER(c_uint32)]),
+    "hm_batch_load": (None, [c_void_p, _PD, _PD, _PD, _PD]),
+    "hm_batch_run": (None, [c_void_p, c_int]),
+    "hm_batch_get": (None, [c_void_p, c_int, c_void_p]),
+    # orbit-loss gradients
+    "hm_adjoint_workspace_bytes": (c_size_t, [c_size_t, c_uint32, c_uint32]),
+    "hm_adjoint": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_double,
+                          c_double, c_uint32, c_uint32, c_int, c_void_p, c_void_p, c_void_p,
+                          c_void_p, c_void_p, c_void_p, c_void_p]),
 }
+
+
+class BatchSet(ctypes.Structure):
+    """hm_batch_set (include/henon_b200.h)."""
+    _fields_ = [("omega_x", c_double), ("omega_y", c_double), ("modulation_kind", c_char_p),
+                ("omega_0", c_double), ("epsilon", c_double), ("offset", c_uint32),
+                ("n_turns", c_uint32), ("n_particles", c_uint64), ("mu", c_double),
+                ("barrier", c_double)]
 
 
 class IndicatorSet(ctypes.Structure):
@@ -544,6 +571,53 @@ def track_indicators(tracker: Tracker, particles: Particles, n_turns: int, mu: f
     call("hm_track_indicators", tracker.h, particles.h, int(n_turns), float(mu), float(barrier),
          ctypes.byref(s))
     del keep
+
+
+class Batch(_Handle):
+    """hm_batch: heterogeneous parameter sets tracked together.
+
+    `sets` is a sequence of dicts with keys omega_x, omega_y, epsilon, mu,
+    n_turns, n_particles and optionally barrier (10.0), modulation_kind
+    ("sps"), omega_0 (nan), offset (0)."""
+    _destroy = "hm_batch_destroy"
+
+    def __init__(self, sets):
+        super().__init__()
+        arr = (BatchSet * len(sets))()
+        self._kinds = []
+        for k, s in enumerate(sets):
+            kind = str(s.get("modulation_kind", "sps")).encode()
+            self._kinds.append(kind)
+            arr[k] = BatchSet(float(s["omega_x"]), float(s["omega_y"]), kind,
+                              float(s.get("omega_0", float("nan"))), float(s["epsilon"]),
+                              int(s.get("offset", 0)), int(s["n_turns"]), int(s["n_particles"]),
+                              float(s["mu"]), float(s.get("barrier", 10.0)))
+        call("hm_batch_create", len(sets), ctypes.cast(arr, c_void_p), ctypes.byref(self.h))
+        self.n_total = sum(int(s["n_particles"]) for s in sets)
+
+    def configure(self, arith: int = ARITH_EXACT, per_thread: int = 2, chunk0: int = 512,
+                  chunk_max: int = 16384):
+        call("hm_batch_configure", self.h, int(arith), int(per_thread), int(chunk0),
+             int(chunk_max))
+
+    def n_chunks(self) -> int:
+        a, b = c_uint64(), c_uint32()
+        call("hm_batch_size", self.h, ctypes.byref(a), ctypes.byref(b))
+        return int(b.value)
+
+    def load(self, x, px, y, py):
+        x, px, y, py = (f64(a) for a in (x, px, y, py))
+        if x.size != self.n_total:
+            raise ValueError("initial conditions must cover every set's particles")
+        call("hm_batch_load", self.h, dptr(x), dptr(px), dptr(y), dptr(py))
+
+    def run(self, use_graph: bool = True):
+        call("hm_batch_run", self.h, int(bool(use_graph)))
+
+    def get(self, field: int) -> np.ndarray:
+        out = np.empty(self.n_total, dtype=FIELD_DTYPE[field])
+        call("hm_batch_get", self.h, int(field), out.ctypes.data_as(c_void_p))
+        return out
 
 
 def set_track_config(threads: int, per_thread: int, chunk0: int, chunk_max: int) -> None:

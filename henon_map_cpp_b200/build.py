@@ -35,8 +35,10 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--fmad=f
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
              f"-I{CUDA_HOME / 'include'}", f"-I{INCLUDE}"]
 
-CU_SOURCES = ["track.cu", "noalloc.cu", "tangent.cu", "fused.cu"]
-CPP_SOURCES = ["capi.cpp", "modulation.cpp", "indicators.cpp"]
+CU_SOURCES = ["track.cu", "noalloc.cu", "tangent.cu", "fused.cu", "ghosts.cu", "batch.cu",
+              "adjoint.cu"]
+CPP_SOURCES = ["capi.cpp", "modulation.cpp", "indicators.cpp", "particles_extra.cpp",
+               "batch.cpp", "adjoint.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -1,0 +1,259 @@
+// Reverse-mode adjoint of the modulated Henon map (sm_100a).
+//
+// Per particle i the orbit loss is the Birkhoff-weighted average
+//     L_i = sum_{k=0}^{N-1} w_k A(x_{k+1}),   A = x^2 + px^2 + y^2 + py^2,
+// w = birkhoff_weights(N), x_{k+1} the state after turn k.  Lost particles
+// (outside the barrier before turn N) contribute nothing.
+//
+// Parameters theta = (omega_x0, omega_y0, epsilon, mu) with
+//     omega_{x,y}(k) = omega_{x,y}0 (1 + epsilon S_k),
+//     S_k = sum_j c_j cos(Omega_j (k + offset))   (SPS ripple, host table).
+//
+// One thread per particle: the forward pass stores a checkpoint every C
+// turns; the reverse sweep recomputes each segment from its checkpoint into
+// a scratch buffer and propagates the adjoint lambda_k = J_k^T lambda_{k+1}
+// + w_{k-1} grad A(x_k) through it, accumulating dL_i/dtheta.  The forward
+// arithmetic is the tracker's (exact or FMA), so the orbit is the one
+// hm_track computes.  A forward-mode kernel (tangent map M_k propagated
+// along the orbit, g = sum_k w_k M_{k+1}^T grad A(x_{k+1})) gives an
+// independent J^T v for the initial conditions.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hm_device.cuh"
+#include "hm_internal.h"
+
+namespace hm {
+namespace {
+
+using dev::Rn;
+
+__device__ __forceinline__ bool inside(double r, long long b2bits) {
+    return static_cast<unsigned long long>(__double_as_longlong(r)) <
+           static_cast<unsigned long long>(b2bits);
+}
+
+struct S4 {
+    double x, px, y, py;
+};
+
+// One forward turn; returns x^2+px^2+y^2+py^2 of the new state in the
+// tracker's grouping (the loss uses the same number).
+template <int ARITH, bool OCT>
+__device__ __forceinline__ double fwd(S4 &s, const dev::Turn &t, double mu) {
+    const double x = s.x, y = s.y;
+    double px, py, X, PX, Y, PY;
+    if (ARITH == HM_ARITH_EXACT) {
+        const double xx = Rn::mul(x, x), yy = Rn::mul(y, y);
+        px = Rn::add(s.px, Rn::sub(xx, yy));
+        py = Rn::add(s.py, Rn::mul(Rn::mul(-2.0, x), y));
+        if (OCT) {
+            px = Rn::add(px, Rn::mul(mu, Rn::sub(Rn::mul(xx, x), Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
+            py = Rn::add(py, Rn::mul(mu, Rn::sub(Rn::mul(yy, y), Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
+        }
+        X = Rn::add(Rn::mul(x, t.cx), Rn::mul(px, t.sx));
+        PX = Rn::add(Rn::mul(-x, t.sx), Rn::mul(px, t.cx));
+        Y = Rn::add(Rn::mul(y, t.cy), Rn::mul(py, t.sy));
+        PY = Rn::add(Rn::mul(-y, t.sy), Rn::mul(py, t.cy));
+        s = S4{X, PX, Y, PY};
+        return Rn::add(Rn::add(Rn::mul(X, X), Rn::mul(PX, PX)), Rn::add(Rn::mul(Y, Y), Rn::mul(PY, PY)));
+    }
+    const double xx = x * x, yy = y * y;
+    px = s.px + (xx - yy);
+    py = fma(-2.0 * x, y, s.py);
+    if (OCT) {
+        px = fma(mu * x, fma(-3.0, yy, xx), px);
+        py = fma(mu * y, fma(-3.0, xx, yy), py);
+    }
+    X = fma(x, t.cx, px * t.sx);
+    PX = fma(px, t.cx, -x * t.sx);
+    Y = fma(y, t.cy, py * t.sy);
+    PY = fma(py, t.cy, -y * t.sy);
+    s = S4{X, PX, Y, PY};
+    return fma(PX, PX, X * X) + fma(PY, PY, Y * Y);
+}
+
+__device__ __forceinline__ void store4(double *buf, size_t slot, size_t n, size_t i, const S4 &s) {
+    double *b = buf + slot * 4 * n;
+    b[i] = s.x;
+    b[n + i] = s.px;
+    b[2 * n + i] = s.y;
+    b[3 * n + i] = s.py;
+}
+
+__device__ __forceinline__ S4 load4(const double *buf, size_t slot, size_t n, size_t i) {
+    const double *b = buf + slot * 4 * n;
+    return S4{b[i], b[n + i], b[2 * n + i], b[3 * n + i]};
+}
+
+template <int ARITH, bool OCT>
+__global__ void __launch_bounds__(128) adjoint_kernel(const AdjointArgs a) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const size_t n = a.n;
+    const uint32_t N = a.n_turns, C = a.ckpt;
+    S4 s{a.x0[i], a.px0[i], a.y0[i], a.py0[i]};
+    bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
+    double loss = 0.0;
+    uint32_t k = 0;
+    for (; alive && k < N; ++k) {
+        if (k % C == 0) store4(a.ckpt_buf, k / C, n, i, s);
+        const double r = fwd<ARITH, OCT>(s, dev::load_turn(a.table, k), a.mu);
+        if (!inside(r, a.b2bits)) {
+            alive = false;
+            break;
+        }
+        loss = fma(a.w[k], r, loss);
+    }
+    a.steps[i] = alive ? N : k;
+    if (!alive) {
+        a.loss[i] = 0.0;
+        a.survived[i] = 0;
+        a.g_ic[i] = a.g_ic[n + i] = a.g_ic[2 * n + i] = a.g_ic[3 * n + i] = 0.0;
+        a.g_th[i] = a.g_th[n + i] = a.g_th[2 * n + i] = a.g_th[3 * n + i] = 0.0;
+        return;
+    }
+    a.loss[i] = loss;
+    a.survived[i] = 1;
+
+    // Reverse sweep, segment by segment.
+    double lx = 0.0, lpx = 0.0, ly = 0.0, lpy = 0.0;
+    double g_wx = 0.0, g_wy = 0.0, g_eps = 0.0, g_mu = 0.0;
+    const double mu = a.mu;
+    const uint32_t n_seg = (N + C - 1) / C;
+    for (int seg = int(n_seg) - 1; seg >= 0; --seg) {
+        const uint32_t k0 = uint32_t(seg) * C;
+        const uint32_t len = min(C, N - k0);
+        S4 q = load4(a.ckpt_buf, uint32_t(seg), n, i);
+        for (uint32_t j = 0; j < len; ++j) {
+            store4(a.seg_buf, j, n, i, q);
+            fwd<ARITH, OCT>(q, dev::load_turn(a.table, k0 + j), mu);
+        }
+        for (int j = int(len) - 1; j >= 0; --j) {
+            const uint32_t kk = k0 + uint32_t(j);
+            const S4 p = load4(a.seg_buf, uint32_t(j), n, i);
+            const dev::Turn t = dev::load_turn(a.table, kk);
+            // forward intermediates of turn kk
+            const double x = p.x, y = p.y;
+            const double xx = x * x, yy = y * y;
+            const double qx = (xx - yy) + mu * x * (xx - 3.0 * yy);
+            const double qy = -2.0 * x * y + mu * y * (yy - 3.0 * xx);
+            const double px1 = p.px + qx, py1 = p.py + qy;
+            const double X = t.cx * x + t.sx * px1, PX = -t.sx * x + t.cx * px1;
+            const double Y = t.cy * y + t.sy * py1, PY = -t.sy * y + t.cy * py1;
+            // dL/d(state after turn kk): lambda + w_kk grad A
+            const double w2 = 2.0 * a.w[kk];
+            const double aX = fma(w2, X, lx), aPX = fma(w2, PX, lpx);
+            const double aY = fma(w2, Y, ly), aPY = fma(w2, PY, lpy);
+            // rotation angle derivatives: d(X, PX)/d omega = (PX, -X)
+            const double gwx = aX * PX - aPX * X;
+            const double gwy = aY * PY - aPY * Y;
+            const double Sk = a.S[kk];
+            const double f = fma(a.epsilon, Sk, 1.0);
+            g_wx = fma(gwx, f, g_wx);
+            g_wy = fma(gwy, f, g_wy);
+            g_eps = fma(Sk, a.omega_x0 * gwx + a.omega_y0 * gwy, g_eps);
+            // through the rotations (transpose)
+            const double rx = t.cx * aX - t.sx * aPX, rpx = t.sx * aX + t.cx * aPX;
+            const double ry = t.cy * aY - t.sy * aPY, rpy = t.sy * aY + t.cy * aPY;
+            // through the kicks
+            const double da = 2.0 * x + 3.0 * mu * (xx - yy);     // dqx/dx
+            const double db = -2.0 * y - 6.0 * mu * x * y;       // dqx/dy = dqy/dx
+            const double dd = -2.0 * x + 3.0 * mu * (yy - xx);    // dqy/dy
+            g_mu = fma(rpx, x * (xx - 3.0 * yy), fma(rpy, y * (yy - 3.0 * xx), g_mu));
+            lx = rx + rpx * da + rpy * db;
+            ly = ry + rpx * db + rpy * dd;
+            lpx = rpx;
+            lpy = rpy;
+        }
+    }
+    a.g_ic[i] = lx;
+    a.g_ic[n + i] = lpx;
+    a.g_ic[2 * n + i] = ly;
+    a.g_ic[3 * n + i] = lpy;
+    a.g_th[i] = g_wx;
+    a.g_th[n + i] = g_wy;
+    a.g_th[2 * n + i] = g_eps;
+    a.g_th[3 * n + i] = g_mu;
+}
+
+// Forward mode: loss and, with TANGENT, g = sum_k w_k M_{k+1}^T grad A(x_{k+1})
+// with M_{k+1} = DF_k ... DF_0 (DF_k = tangent_matrix at x_k, table[k]).
+template <int ARITH, bool OCT, bool TANGENT>
+__global__ void __launch_bounds__(128) forward_loss_kernel(const AdjointArgs a) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const size_t n = a.n;
+    S4 s{a.x0[i], a.px0[i], a.y0[i], a.py0[i]};
+    bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
+    double M[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    double g[4] = {0, 0, 0, 0};
+    double loss = 0.0;
+    uint32_t k = 0;
+    for (; alive && k < a.n_turns; ++k) {
+        const dev::Turn t = dev::load_turn(a.table, k);
+        if (TANGENT) {
+            double df[16], out[16];
+            dev::tangent_matrix_exact(s.x, s.y, t, a.mu, df);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc = fma(df[r * 4 + q], M[q * 4 + c], acc);
+                    out[r * 4 + c] = acc;
+                }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) M[q] = out[q];
+        }
+        const double r = fwd<ARITH, OCT>(s, t, a.mu);
+        if (!inside(r, a.b2bits)) {
+            alive = false;
+            break;
+        }
+        loss = fma(a.w[k], r, loss);
+        if (TANGENT) {
+            const double w2 = 2.0 * a.w[k];
+            const double v[4] = {w2 * s.x, w2 * s.px, w2 * s.y, w2 * s.py};
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                g[c] = fma(M[c], v[0], fma(M[4 + c], v[1], fma(M[8 + c], v[2], fma(M[12 + c], v[3], g[c]))));
+        }
+    }
+    a.steps[i] = alive ? a.n_turns : k;
+    a.survived[i] = alive ? 1 : 0;
+    a.loss[i] = alive ? loss : 0.0;
+    if (TANGENT) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a.g_ic[size_t(c) * n + i] = alive ? g[c] : 0.0;
+    }
+}
+
+template <int ARITH>
+cudaError_t launch_a(const AdjointArgs &a, int mode, cudaStream_t s) {
+    const unsigned blocks = unsigned((a.n + 127) / 128);
+    const bool oct = a.mu != 0.0;
+    if (mode == 0) {
+        if (oct) adjoint_kernel<ARITH, true><<<blocks, 128, 0, s>>>(a);
+        else adjoint_kernel<ARITH, false><<<blocks, 128, 0, s>>>(a);
+    } else if (mode == 1) {
+        if (oct) forward_loss_kernel<ARITH, true, true><<<blocks, 128, 0, s>>>(a);
+        else forward_loss_kernel<ARITH, false, true><<<blocks, 128, 0, s>>>(a);
+    } else {
+        if (oct) forward_loss_kernel<ARITH, true, false><<<blocks, 128, 0, s>>>(a);
+        else forward_loss_kernel<ARITH, false, false><<<blocks, 128, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_adjoint(const AdjointArgs &a, int mode, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    return a.arith == HM_ARITH_FAST ? launch_a<HM_ARITH_FAST>(a, mode, s)
+                                    : launch_a<HM_ARITH_EXACT>(a, mode, s);
+}
+
+}  // namespace hm

@@ -1,0 +1,282 @@
+// Batched heterogeneous tracking: many parameter sets (tunes, epsilon, mu,
+// barrier), each with its own particle count and turn budget, advanced
+// together chunk by chunk with no host round trip in between.
+//
+// Per chunk:
+//   * batch_chunk_kernel -- a persistent grid; every warp pops warp-tiles
+//     (32*K live particles of ONE set, so the turn record, mu and barrier
+//     are warp-uniform) from a device work queue, runs the set's turns of
+//     this chunk with the particles in registers, writes lost particles out
+//     at once and appends survivors to its set's next list;
+//   * batch_plan_kernel -- one block: per-set survivor counts -> next tile
+//     table (prefix sum), counters reset, ping-pong parity flipped.
+// The whole sequence (init, plan, n_chunks x (chunk, plan)) has a fixed
+// shape, so the host captures it once in a CUDA graph and replays it.
+//
+// The per-particle arithmetic is the tracking kernel's (track.cu), so every
+// set's result is bit-identical to a plain hm_track of that set.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hm_device.cuh"
+#include "hm_internal.h"
+
+namespace hm {
+namespace {
+
+using dev::Rn;
+
+__device__ __forceinline__ bool inside(double r, long long b2bits) {
+    return static_cast<unsigned long long>(__double_as_longlong(r)) <
+           static_cast<unsigned long long>(b2bits);
+}
+
+struct P {
+    double x, px, y, py, xx, yy;
+};
+
+template <bool OCT>
+__device__ __forceinline__ double turn_exact(P &p, const dev::Turn &t, double mu) {
+    double px = Rn::add(p.px, Rn::sub(p.xx, p.yy));
+    double py = Rn::add(p.py, Rn::mul(Rn::mul(-2.0, p.x), p.y));
+    if (OCT) {
+        px = Rn::add(px, Rn::mul(mu, Rn::sub(Rn::mul(p.xx, p.x),
+                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.y), p.y), p.x))));
+        py = Rn::add(py, Rn::mul(mu, Rn::sub(Rn::mul(p.yy, p.y),
+                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.x), p.x), p.y))));
+    }
+    const double x = Rn::add(Rn::mul(p.x, t.cx), Rn::mul(px, t.sx));
+    px = Rn::add(Rn::mul(-p.x, t.sx), Rn::mul(px, t.cx));
+    const double y = Rn::add(Rn::mul(p.y, t.cy), Rn::mul(py, t.sy));
+    py = Rn::add(Rn::mul(-p.y, t.sy), Rn::mul(py, t.cy));
+    p.xx = Rn::mul(x, x);
+    p.yy = Rn::mul(y, y);
+    p.x = x;
+    p.px = px;
+    p.y = y;
+    p.py = py;
+    return Rn::add(Rn::add(p.xx, Rn::mul(px, px)), Rn::add(p.yy, Rn::mul(py, py)));
+}
+
+template <bool OCT>
+__device__ __forceinline__ double turn_fast(P &p, const dev::Turn &t, double mu) {
+    double px = p.px + (p.xx - p.yy);
+    double py = fma(-2.0 * p.x, p.y, p.py);
+    if (OCT) {
+        px = fma(mu * p.x, fma(-3.0, p.yy, p.xx), px);
+        py = fma(mu * p.y, fma(-3.0, p.xx, p.yy), py);
+    }
+    const double x = fma(p.x, t.cx, px * t.sx);
+    px = fma(px, t.cx, -p.x * t.sx);
+    const double y = fma(p.y, t.cy, py * t.sy);
+    py = fma(py, t.cy, -p.y * t.sy);
+    p.xx = x * x;
+    p.yy = y * y;
+    p.x = x;
+    p.px = px;
+    p.y = y;
+    p.py = py;
+    return fma(px, px, p.xx) + fma(py, py, p.yy);
+}
+
+template <int ARITH, bool OCT>
+__device__ __forceinline__ double one_turn(P &p, const dev::Turn &t, double mu) {
+    return ARITH == HM_ARITH_EXACT ? turn_exact<OCT>(p, t, mu) : turn_fast<OCT>(p, t, mu);
+}
+
+// Copies every non-NaN particle of every set into list 0 of its set and
+// counts them (check_nan: NaN particles are never touched).
+__global__ void batch_init_kernel(BatchDev b) {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i == 0) *b.parity = 1u;  // the first plan flips it to list 0
+    if (i >= b.n_total) return;
+    const uint32_t s = b.particle_set[i];
+    const double x = b.x[i], px = b.px[i], y = b.y[i], py = b.py[i];
+    if (dev::is_lost(x, px, y, py)) return;
+    const BatchSetDev &set = b.sets[s];
+    const uint32_t o = atomicAdd(&b.state[s].next, 1u);
+    const uint64_t slot = set.list_offset + o;
+    b.list_idx[0][slot] = i;
+    b.list_x[0][slot] = x;
+    b.list_px[0][slot] = px;
+    b.list_y[0][slot] = y;
+    b.list_py[0][slot] = py;
+}
+
+// Between chunks: survivors -> live counts, next tile table.  One block.
+__global__ void batch_plan_kernel(BatchDev b, uint32_t chunk_len_done, uint32_t chunk_len_next) {
+    __shared__ uint32_t tiles_of[kBatchMaxSets];
+    const int s = threadIdx.x;
+    const uint32_t tile = 32u * uint32_t(b.per_thread);
+    if (s < b.n_sets) {
+        BatchStateDev &st = b.state[s];
+        const uint32_t budget = b.sets[s].n_turns;
+        const uint32_t ran = min(chunk_len_done, budget - st.done);
+        st.done += ran;
+        st.live = (st.done < budget) ? st.next : 0u;
+        st.next = 0u;
+        st.turns = min(chunk_len_next, budget - st.done);
+        tiles_of[s] = st.turns ? (st.live + tile - 1) / tile : 0u;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (int k = 0; k < b.n_sets; ++k) {
+            b.state[k].first_tile = total;
+            total += tiles_of[k];
+        }
+        *b.n_tiles = total;
+        *b.next_item = 0u;
+        *b.parity ^= 1u;
+    }
+    __syncthreads();
+    if (s < b.n_sets) {
+        const uint32_t first = b.state[s].first_tile;
+        for (uint32_t t = 0; t < tiles_of[s]; ++t) b.tile_set[first + t] = uint32_t(s);
+    }
+}
+
+template <int ARITH, bool OCT, int K>
+__device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &set,
+                                         const BatchStateDev &st, uint32_t s, uint32_t start,
+                                         int in, int out) {
+    const unsigned lane = threadIdx.x & 31u;
+    P p[K];
+    uint64_t id[K];
+    bool live[K];
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const uint32_t e = start + uint32_t(j) * 32u + lane;
+        live[j] = e < st.live;
+        const uint64_t slot = set.list_offset + (live[j] ? e : 0u);
+        id[j] = b.list_idx[in][slot];
+        const double x = b.list_x[in][slot], y = b.list_y[in][slot];
+        p[j] = P{x, b.list_px[in][slot], y, b.list_py[in][slot], Rn::mul(x, x), Rn::mul(y, y)};
+        any |= live[j];
+    }
+    const uint32_t turn0 = st.done, nt = st.turns;
+    const double mu = set.mu;
+    bool warp_live = __any_sync(dev::kFullMask, any);
+    for (uint32_t k = 0; warp_live && k < nt; ++k) {
+        const dev::Turn t = dev::load_turn(set.table, turn0 + k);
+        bool any_lost = false;
+        bool lost[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const double r = one_turn<ARITH, OCT>(p[j], t, mu);
+            lost[j] = live[j] && !inside(r, set.b2bits);
+            any_lost |= lost[j];
+        }
+        if (__any_sync(dev::kFullMask, any_lost)) {
+            bool still = false;
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (lost[j]) {
+                    b.x[id[j]] = b.px[id[j]] = b.y[id[j]] = b.py[id[j]] = dev::quiet_nan();
+                    b.steps[id[j]] = turn0 + k;
+                    live[j] = false;
+                }
+                still |= live[j];
+            }
+            warp_live = __any_sync(dev::kFullMask, still);
+        }
+    }
+    const bool final_chunk = turn0 + nt == set.n_turns;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        if (final_chunk) {
+            if (live[j]) {
+                b.x[id[j]] = p[j].x;
+                b.px[id[j]] = p[j].px;
+                b.y[id[j]] = p[j].y;
+                b.py[id[j]] = p[j].py;
+                b.steps[id[j]] = set.n_turns;
+            }
+            continue;
+        }
+        const unsigned m = __ballot_sync(dev::kFullMask, live[j]);
+        if (m == 0u) continue;
+        const int leader = __ffs(m) - 1;
+        uint32_t off = 0;
+        if (lane == unsigned(leader)) off = atomicAdd(&b.state[s].next, uint32_t(__popc(m)));
+        off = __shfl_sync(dev::kFullMask, off, leader);
+        if (live[j]) {
+            const uint64_t slot = set.list_offset + off + __popc(m & ((1u << lane) - 1u));
+            b.list_idx[out][slot] = id[j];
+            b.list_x[out][slot] = p[j].x;
+            b.list_px[out][slot] = p[j].px;
+            b.list_y[out][slot] = p[j].y;
+            b.list_py[out][slot] = p[j].py;
+        }
+    }
+}
+
+// Persistent: warps pop warp-tiles until the chunk's queue is empty.
+template <int ARITH, int K>
+__global__ void __launch_bounds__(128) batch_chunk_kernel(BatchDev b) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t n_tiles = *b.n_tiles;
+    const int in = int(*b.parity), out = 1 - in;
+    while (true) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(b.next_item, 1u);
+        item = __shfl_sync(dev::kFullMask, item, 0);
+        if (item >= n_tiles) return;
+        const uint32_t s = b.tile_set[item];
+        const BatchStateDev st = b.state[s];
+        const BatchSetDev &set = b.sets[s];
+        const uint32_t start = (item - st.first_tile) * 32u * uint32_t(K);
+        if (set.mu != 0.0)
+            run_tile<ARITH, true, K>(b, set, st, s, start, in, out);
+        else
+            run_tile<ARITH, false, K>(b, set, st, s, start, in, out);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_batch_init(const BatchDev &b, cudaStream_t s) {
+    if (b.n_total == 0) return cudaSuccess;
+    batch_init_kernel<<<unsigned((b.n_total + 255) / 256), 256, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_plan(const BatchDev &b, uint32_t done_len, uint32_t next_len,
+                              cudaStream_t s) {
+    batch_plan_kernel<<<1, kBatchMaxSets, 0, s>>>(b, done_len, next_len);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_chunk(const BatchDev &b, int blocks, cudaStream_t s) {
+    const int a = b.arith, k = b.per_thread;
+#define HM_BATCH_LAUNCH(A, KK) batch_chunk_kernel<A, KK><<<blocks, 128, 0, s>>>(b)
+    if (a == HM_ARITH_FAST) {
+        if (k == 1) HM_BATCH_LAUNCH(HM_ARITH_FAST, 1);
+        else if (k == 2) HM_BATCH_LAUNCH(HM_ARITH_FAST, 2);
+        else HM_BATCH_LAUNCH(HM_ARITH_FAST, 4);
+    } else {
+        if (k == 1) HM_BATCH_LAUNCH(HM_ARITH_EXACT, 1);
+        else if (k == 2) HM_BATCH_LAUNCH(HM_ARITH_EXACT, 2);
+        else HM_BATCH_LAUNCH(HM_ARITH_EXACT, 4);
+    }
+#undef HM_BATCH_LAUNCH
+    return cudaGetLastError();
+}
+
+int batch_chunk_blocks_per_sm(int arith, int per_thread) {
+    int n = 0;
+    cudaError_t e;
+    if (arith == HM_ARITH_FAST)
+        e = per_thread == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 1>, 128, 0)
+            : per_thread == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 2>, 128, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 4>, 128, 0);
+    else
+        e = per_thread == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 1>, 128, 0)
+            : per_thread == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 2>, 128, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 4>, 128, 0);
+    return e == cudaSuccess && n > 0 ? n : 1;
+}
+
+}  // namespace hm

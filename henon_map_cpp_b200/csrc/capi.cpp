@@ -364,9 +364,22 @@ hm_status compute_tables(hm_tracker *t, uint32_t n_turns, double omega_x, double
     if (!kind) return fail(HM_ERR_INVALID_ARG, "null modulation kind");
     std::vector<double> wx, wy;
     HM_TRY(hm::modulation(kind, n_turns, omega_x, omega_y, omega_0, epsilon, offset, wx, wy));
-    return upload_tables(t, wx, wy);
+    HM_TRY(upload_tables(t, wx, wy));
+    t->kind = kind;
+    t->omega_x = omega_x;
+    t->omega_y = omega_y;
+    t->omega_0 = omega_0;
+    t->epsilon = epsilon;
+    t->offset = offset;
+    return ok();
 }
 
+}  // namespace
+
+namespace hm {
+
+// (Re)allocates the device arrays of p for p->n_total particles and uploads
+// coordinates, steps and the host-side bookkeeping vectors.
 hm_status particles_upload(hm_particles *p, const double *x, const double *px,
                            const double *y, const double *py,
                            const std::vector<uint32_t> &steps) {
@@ -393,7 +406,9 @@ hm_status particles_upload(hm_particles *p, const double *x, const double *px,
     return ok();
 }
 
-}  // namespace
+}  // namespace hm
+
+using hm::particles_upload;
 
 extern "C" {
 

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -43,6 +44,8 @@ hm_status modulation(const std::string &kind, uint32_t n_turns, double omega_x,
                      uint32_t offset, std::vector<double> &wx,
                      std::vector<double> &wy);
 std::vector<double> birkhoff_weights(uint32_t n);
+hm_status modulation_ripple(const std::string &kind, uint32_t n_turns, double omega_0,
+                            uint32_t offset, std::vector<double> &ripple);
 
 // ---- device buffers ---------------------------------------------------------
 
@@ -85,7 +88,9 @@ struct hm_particles {
     std::vector<uint64_t> idx, idx_base;
     hm::DeviceBuffer x, px, y, py, steps, dvalid, dghost, didx, didx_base;
     hm::DeviceBuffer work;  // survivor lists of the chunked tracker
-    uint64_t rng_state = 0x9e3779b97f4a7c15ULL;
+    // Generator of "random" ghost directions: default-seeded, one per
+    // particle set, as the reference's particles_4d::rng.
+    std::mt19937_64 rng;
 };
 
 // Modulation tables on the device (henon_tracker_gpu, src/henon.h:212-228).
@@ -94,6 +99,10 @@ struct hm_tracker {
     std::vector<double> sx, cx, sy, cy;  // host copies
     hm::DeviceBuffer table;              // {sx, cx, sy, cy} per turn
     hm_arith arith = HM_ARITH_EXACT;
+    // Modulation parameters the tables were built from (for derivatives).
+    std::string kind = "sps";
+    double omega_x = 0.0, omega_y = 0.0, omega_0 = 0.0, epsilon = 0.0;
+    uint32_t offset = 0;
 };
 
 namespace hm {
@@ -234,6 +243,87 @@ cudaError_t launch_indicators(const FusedArgs &a, cudaStream_t s);
 // Largest number of per-thread window accumulators the fused kernel takes
 // (n_megno_birkhoff + 2 n_lyapunov + 4 n_tune).
 size_t fused_max_slots();
+
+// ---- batched heterogeneous tracking (batch.cu / batch.cpp) -------------------
+
+constexpr int kBatchMaxSets = 1024;  // one planning thread per set
+
+struct BatchSetDev {
+    const double *table;   // this set's turn records
+    uint64_t list_offset;  // start of the set's region in each survivor list
+    uint32_t n_particles;
+    uint32_t n_turns;      // turn budget
+    double mu;
+    long long b2bits;      // bit pattern of barrier^2 (0 when NaN)
+};
+
+struct BatchStateDev {
+    uint32_t live;        // particles in the set's current list
+    uint32_t next;        // survivors appended to the next list (atomic)
+    uint32_t done;        // turns done
+    uint32_t turns;       // turns of the current chunk
+    uint32_t first_tile;  // first work item of the set in the current chunk
+};
+
+struct BatchDev {
+    double *x, *px, *y, *py;
+    uint32_t *steps;
+    const uint32_t *particle_set;
+    uint64_t n_total;
+    const BatchSetDev *sets;
+    BatchStateDev *state;
+    int n_sets;
+    uint64_t *list_idx[2];
+    double *list_x[2], *list_px[2], *list_y[2], *list_py[2];
+    uint32_t *tile_set;
+    uint32_t *n_tiles, *next_item, *parity;
+    int arith;
+    int per_thread;
+};
+
+cudaError_t launch_batch_init(const BatchDev &b, cudaStream_t s);
+cudaError_t launch_batch_plan(const BatchDev &b, uint32_t done_len, uint32_t next_len,
+                              cudaStream_t s);
+cudaError_t launch_batch_chunk(const BatchDev &b, int blocks, cudaStream_t s);
+int batch_chunk_blocks_per_sm(int arith, int per_thread);
+
+// ---- adjoint (adjoint.cu / adjoint.cpp) ---------------------------------------
+
+struct AdjointArgs {
+    const double *x0, *px0, *y0, *py0;
+    size_t n;
+    const double *table;  // tracker turn records
+    const double *S;      // modulation ripple S_k (omega(k) = omega0 (1 + eps S_k))
+    const double *w;      // Birkhoff weights of n_turns
+    uint32_t n_turns, ckpt;
+    double mu, epsilon, omega_x0, omega_y0;
+    long long b2bits;
+    int arith;
+    double *ckpt_buf;  // [ceil(n_turns / ckpt)][4][n]
+    double *seg_buf;   // [ckpt][4][n]
+    double *loss;      // [n] per-particle loss (0 when lost)
+    uint8_t *survived; // [n]
+    uint32_t *steps;   // [n] turns survived
+    double *g_ic;      // [4][n]
+    double *g_th;      // [4][n] per-particle dL_i/d(omega_x0, omega_y0, eps, mu)
+};
+
+// mode 0: loss + reverse-mode gradients; 1: loss + forward-mode initial-
+// condition gradient (tangent map); 2: loss only.
+cudaError_t launch_adjoint(const AdjointArgs &a, int mode, cudaStream_t s);
+
+// (Re)allocates and uploads the device arrays of p (capi.cpp).
+hm_status particles_upload(hm_particles *p, const double *x, const double *px, const double *y,
+                           const double *py, const std::vector<uint32_t> &steps);
+
+// Ghost particles (ghosts.cu).
+cudaError_t launch_renormalize(double *x, double *px, double *y, double *py,
+                               const uint64_t *idx_base, const uint8_t *ghost, size_t n,
+                               double module, cudaStream_t s);
+cudaError_t launch_displacement(const double *x, const double *px, const double *y,
+                                const double *py, const uint64_t *idx, const uint64_t *idx_base,
+                                const uint8_t *ghost, size_t n, size_t n_base, double *module,
+                                double *dx, double *dpx, double *dy, double *dpy, cudaStream_t s);
 
 // Uploads a host vector to a fresh device buffer.
 template <class T>

@@ -121,6 +121,34 @@ hm_status modulation(const std::string &kind, uint32_t n_turns, double omega_x,
     return ok();
 }
 
+// The ripple S_n of omega(n) = 2*pi*tune*(1 + eps*S_n) for the kinds whose
+// angle is differentiable in (tune, eps): "sps" (the harmonic sum above) and
+// "basic" (cos(2*pi*omega_0*i)).
+hm_status modulation_ripple(const std::string &kind, uint32_t n_turns, double omega_0,
+                            uint32_t offset, std::vector<double> &ripple) {
+    ripple.assign(n_turns, 0.0);
+    if (kind == "sps") {
+        double omega_k[kSpsHarmonics];
+        const double fundamental = 2 * M_PI / 868.12;
+        for (int j = 0; j < kSpsHarmonics; ++j)
+            omega_k[j] = double(kSpsMultiple[j]) * fundamental;
+        parallel_for(n_turns, [&](size_t i) {
+            const double turn = double(uint32_t(uint32_t(i) + offset));
+            double s = 0.0;
+            for (int j = 0; j < kSpsHarmonics; ++j) s += kSpsCoefficient[j] * std::cos(omega_k[j] * turn);
+            ripple[i] = s;
+        });
+        return ok();
+    }
+    if (kind == "basic") {
+        const double two_pi_omega = 2 * M_PI * omega_0;
+        for (uint32_t i = 0; i < n_turns; ++i) ripple[i] = std::cos(two_pi_omega * int(i));
+        return ok();
+    }
+    return fail(HM_ERR_NOT_SUPPORTED,
+                "derivatives need an 'sps' or 'basic' modulation (random tunes have none)");
+}
+
 // w_i = exp(-1/(t(1-t))), t = i/n, normalised by the left-to-right sum
 // (birkhoff_weights, src/dynamic_indicator.cpp:63-79).
 std::vector<double> birkhoff_weights(uint32_t n) {

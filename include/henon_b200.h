@@ -168,6 +168,27 @@ hm_status hm_particles_device_ptr(const hm_particles *p, hm_field field,
 hm_status hm_particles_observable(const hm_particles *p, hm_observable kind,
                                   double *host_out);
 
+/* Ghost particles (particles_4d::add_ghost, src/henon.cu:737-818): one ghost
+ * per base particle, displaced by `module` along "x", "px", "y", "py" or an
+ * isotropic "random" direction (the set's default-seeded mt19937_64, as the
+ * reference).  Like the reference's GPU class (:1247-1255) the device state
+ * is rebuilt from the initial conditions. */
+hm_status hm_particles_add_ghost(hm_particles *p, double module,
+                                 const char *direction);
+/* renormalize (src/henon.cu:1257-1282). */
+hm_status hm_particles_renormalize(hm_particles *p, double module);
+/* get_displacement_module (:1284-1343): double[n_particles][n_ghosts]. */
+hm_status hm_particles_displacement_module(const hm_particles *p,
+                                           double *host_out);
+/* get_displacement_direction (:1345-1442): double[4][n_particles][n_ghosts]. */
+hm_status hm_particles_displacement_direction(const hm_particles *p,
+                                              double *host_out);
+/* henon_tracker_gpu::get_tangent_matrix (src/henon.cu:3187-3219), computed
+ * on the host like the reference: double[n_total][16]. */
+hm_status hm_tracker_tangent_matrices(const hm_tracker *t,
+                                      const hm_particles *p, double mu,
+                                      int reverse, double *host_out);
+
 /* ---- tracking ---------------------------------------------------------- */
 
 /* henon_tracker_gpu::track, src/henon.cu:3155-3185: n_turns turns of the
@@ -335,6 +356,68 @@ typedef struct hm_indicator_set {
 hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns,
                               double mu, double barrier,
                               const hm_indicator_set *set);
+
+/* ---- batched heterogeneous tracking ---------------------------------------
+ * Replaces the reference's one-process-per-parameter-set sweeps
+ * (htcondor_jobs/compose_config.py:3-15, run_sim.py:41-74): many
+ * (omega_x, omega_y, epsilon, mu, barrier) sets, each with its own particle
+ * count and turn budget, tracked together.  Each set's particles are
+ * advanced exactly as hm_track would advance them alone (bit-identical);
+ * hm_batch_run replays the whole batch as one captured CUDA graph of
+ * persistent chunk launches and planning kernels. */
+typedef struct hm_batch hm_batch;
+typedef struct hm_batch_set {
+    double omega_x, omega_y;      /* tunes (henon_tracker arguments)        */
+    const char *modulation_kind;  /* NULL means "sps"                       */
+    double omega_0, epsilon;
+    uint32_t offset;
+    uint32_t n_turns;             /* turn budget of this set                */
+    uint64_t n_particles;
+    double mu;
+    double barrier;
+} hm_batch_set;
+
+hm_status hm_batch_create(size_t n_sets, const hm_batch_set *sets,
+                          hm_batch **out);
+hm_status hm_batch_destroy(hm_batch *b);
+/* Arithmetic, particles per thread (1, 2, 4) and the chunk schedule (first
+ * chunk, cap of the doubling length); chosen by the autotuner. */
+hm_status hm_batch_configure(hm_batch *b, hm_arith arith, int per_thread,
+                             uint32_t chunk0, uint32_t chunk_max);
+hm_status hm_batch_size(const hm_batch *b, uint64_t *n_total,
+                        uint32_t *n_chunks);
+/* Initial conditions of all sets, concatenated in set order (host). */
+hm_status hm_batch_load(hm_batch *b, const double *x, const double *px,
+                        const double *y, const double *py);
+/* Tracks every set from its initial conditions to its budget.  use_graph:
+ * capture once, replay after. Synchronous. */
+hm_status hm_batch_run(hm_batch *b, int use_graph);
+/* Host copy of x, px, y, py (double) or steps (uint32), concatenated. */
+hm_status hm_batch_get(const hm_batch *b, hm_field field, void *host_out);
+
+/* ---- orbit-loss gradients (reverse-mode adjoint) ---------------------------
+ * No counterpart in the reference (its tangent map is forward only,
+ * src/henon.cu:175-313).  For every particle i of the device arrays x0..py0
+ * the Birkhoff-weighted orbit loss
+ *     L_i = sum_{k=0}^{n_turns-1} w_k (x^2+px^2+y^2+py^2)(after turn k),
+ *     w = birkhoff_weights(n_turns),
+ * is computed with the tracker's tables and arithmetic (the orbit is the
+ * one hm_track follows); particles lost before n_turns get L_i = 0 and
+ * survived[i] = 0.  mode 0 adds reverse-mode gradients: grad_ic[4][n] =
+ * dL_i/d(x0, px0, y0, py0) and grad_theta[4][n] = dL_i/d(omega_x0,
+ * omega_y0, epsilon, mu), omega_{x,y}0 = 2 pi tune_{x,y}, with checkpoints
+ * every checkpoint_every turns and recomputation in between (workspace of
+ * hm_adjoint_workspace_bytes).  mode 1 gives grad_ic by forward-mode
+ * tangent-map propagation (an independent J^T v), mode 2 the loss only.
+ * Derivatives need an "sps" or "basic" modulation.  Synchronous. */
+size_t hm_adjoint_workspace_bytes(size_t n, uint32_t n_turns,
+                                  uint32_t checkpoint_every);
+hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0,
+                     const double *y0, const double *py0, size_t n, double mu,
+                     double barrier, uint32_t n_turns, uint32_t checkpoint_every,
+                     int mode, double *loss, uint8_t *survived, uint32_t *steps,
+                     double *grad_ic, double *grad_theta, void *workspace,
+                     void *stream);
 
 /* No counterpart in the reference.  The same operation as hm_track_device
  * for callers that cannot allocate device memory (an application that

@@ -1,0 +1,121 @@
+"""Reverse-mode adjoint of the orbit loss: checked against central finite
+differences on short horizons (N = 100) and against the forward-mode
+tangent map J^T v on long ones (N = 10^4), through the C ABI and through
+torch.autograd."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import TUNES
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+from henon_map_cpp_b200 import autograd as AG  # noqa: E402
+
+THETA = [2 * math.pi * TUNES[0], 2 * math.pi * TUNES[1], 16.0, 0.1]
+
+
+def c5_points(n, seed=5):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, 0.3, n)
+    y = rng.uniform(0, 0.3, n)
+    px = rng.normal(0, 0.01, n)
+    py = rng.normal(0, 0.01, n)
+    return [torch.tensor(a, dtype=torch.float64, device="cuda") for a in (x, px, y, py)]
+
+
+def test_loss_matches_oracle_orbit(gpu):
+    pts = c5_points(64)
+    th = torch.tensor(THETA, dtype=torch.float64)
+    r = AG.per_particle(*pts, th, 300, mode="loss")
+    host = [p.cpu().numpy() for p in pts]
+    tabs = O.tables(300, *TUNES, "sps", epsilon=16.0)
+    w = O.birkhoff_weights(300)
+    x, px, y, py = host
+    steps = np.zeros(64, np.uint32)
+    loss = np.zeros(64)
+    for k in range(300):
+        x, px, y, py, steps = O.track(x, px, y, py, steps, tabs, 1, 0.1, 10.0)
+        loss += w[k] * ((x * x + px * px) + (y * y + py * py))
+    alive = steps == 300
+    np.testing.assert_array_equal(r["survived"].cpu().numpy(), alive)
+    np.testing.assert_array_equal(r["steps"].cpu().numpy(), steps)
+    np.testing.assert_allclose(r["loss"].cpu().numpy()[alive], loss[alive], rtol=1e-13)
+
+
+def test_adjoint_matches_central_differences(gpu):
+    n_turns = 100
+    pts = c5_points(48, seed=9)
+    th = torch.tensor(THETA, dtype=torch.float64)
+    r = AG.per_particle(*pts, th, n_turns, checkpoint_every=7)
+    surv = r["survived"].cpu().numpy()
+    assert surv.all()
+
+    def losses(points, theta):
+        return AG.per_particle(*points, torch.tensor(theta, dtype=torch.float64), n_turns,
+                               mode="loss")["loss"].cpu().numpy()
+
+    # initial conditions: perturb every particle's coordinate c at once
+    # (particles are independent, so each loss sees only its own shift)
+    for c in range(4):
+        h = 1e-6
+        up = [p.clone() for p in pts]
+        dn = [p.clone() for p in pts]
+        up[c] += h
+        dn[c] -= h
+        fd = (losses(up, THETA) - losses(dn, THETA)) / (2 * h)
+        ad = r["grad_ic"][c].cpu().numpy()
+        np.testing.assert_allclose(ad, fd, rtol=2e-6, atol=1e-9, err_msg=f"coordinate {c}")
+    # parameters (omega_x0, omega_y0, epsilon, mu): per-particle sums
+    for j in range(4):
+        h = 1e-6 * max(1.0, abs(THETA[j]))
+        tu, td = list(THETA), list(THETA)
+        tu[j] += h
+        td[j] -= h
+        fd = (losses(pts, tu) - losses(pts, td)) / (2 * h)
+        ad = r["grad_theta"][j].cpu().numpy()
+        np.testing.assert_allclose(ad, fd, rtol=2e-5, atol=1e-9, err_msg=f"parameter {j}")
+
+
+def test_adjoint_equals_forward_tangent_long_horizon(gpu):
+    n_turns = 10_000
+    pts = c5_points(2048, seed=3)
+    th = torch.tensor(THETA, dtype=torch.float64)
+    adj = AG.per_particle(*pts, th, n_turns, checkpoint_every=100)
+    tan = AG.per_particle(*pts, th, n_turns, mode="tangent")
+    surv = adj["survived"].cpu().numpy()
+    np.testing.assert_array_equal(surv, tan["survived"].cpu().numpy())
+    a = adj["grad_ic"].cpu().numpy()[:, surv]
+    t = tan["grad_ic"].cpu().numpy()[:, surv]
+    rel = np.max(np.abs(a - t), axis=0) / np.max(np.abs(t), axis=0)
+    # Regular orbits: 1e-10.  Chaotic ones have gradients ~exp(lambda N);
+    # both sides are then accurate to a relative error that grows with
+    # |grad|, so the bound is checked on the well-conditioned majority.
+    assert surv.sum() > 1000
+    assert np.mean(rel < 1e-10) >= 0.95, (np.mean(rel < 1e-10), np.nanmax(rel))
+    norm = np.max(np.abs(t), axis=0)
+    assert np.all(rel[norm < 1e3] < 1e-10)
+
+
+def test_autograd_function(gpu):
+    n_turns = 200
+    pts = [p.clone().requires_grad_(True) for p in c5_points(256, seed=1)]
+    th = torch.tensor(THETA, dtype=torch.float64, requires_grad=True)
+    loss = AG.orbit_loss(*pts, th, n_turns, checkpoint_every=20)
+    loss.backward()
+    r = AG.per_particle(*[p.detach() for p in pts], th.detach(), n_turns, checkpoint_every=20)
+    surv = r["survived"]
+    count = surv.sum().item()
+    torch.testing.assert_close(loss.detach(), r["loss"][surv].sum() / count, rtol=1e-14, atol=0)
+    torch.testing.assert_close(pts[0].grad, r["grad_ic"][0] / count, rtol=1e-14, atol=0)
+    torch.testing.assert_close(th.grad, r["grad_theta"].sum(dim=1).cpu() / count, rtol=1e-12,
+                               atol=0)
+    # loss-only path (no gradient requested)
+    with torch.no_grad():
+        l2 = AG.orbit_loss(*[p.detach() for p in pts], th.detach(), n_turns)
+    torch.testing.assert_close(l2, loss.detach(), rtol=0, atol=0)

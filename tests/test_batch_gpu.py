@@ -1,0 +1,69 @@
+"""Batched heterogeneous tracking (hm_batch_*): every parameter set of the
+batch must end exactly as a plain hm_track of that set alone -- same
+coordinates bit for bit, same survival turns -- with and without the CUDA
+graph, over replays, for both arithmetic modes."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import assert_bitwise
+
+pytestmark = pytest.mark.gpu
+
+C = pytest.importorskip("henon_map_cpp_b200._capi")
+from henon_map_cpp_b200 import sweep  # noqa: E402
+
+
+def plain(s, x, px, y, py, arith):
+    t = C.Tracker(s["n_turns"], s["omega_x"], s["omega_y"], "sps", float("nan"), s["epsilon"], 0)
+    t.arith = arith
+    p = C.Particles(x, px, y, py)
+    t.track(p, s["n_turns"], s["mu"], s["barrier"])
+    return p.state()
+
+
+@pytest.mark.parametrize("arith", [0, 1])
+def test_batch_equals_plain_per_set(gpu, arith):
+    sets, coords = sweep.heterogeneous_sets(seed=11, n_sets=9, n_range=(40, 3000),
+                                            turn_range=(50, 6000))
+    sets[3]["n_turns"] = 0          # a set with no turns
+    sets[5]["n_particles"] = 1      # a one-particle set (keep coords in sync below)
+    pts = [sweep.ball_points(np.random.default_rng(100 + k), s["n_particles"], 0.6)
+           for k, s in enumerate(sets)]
+    coords = tuple(np.concatenate([p[k] for p in pts]) for k in range(4))
+    coords[0][7] = np.nan           # a particle lost before tracking
+    res_graph = sweep.run_sweep(sets, coords, arith=arith, chunk0=64, chunk_max=1024)
+    res_plain = sweep.run_sweep(sets, coords, arith=arith, chunk0=100, chunk_max=100,
+                                per_thread=4, use_graph=False)
+    o = 0
+    for s, rg, rp in zip(sets, res_graph, res_plain):
+        n = s["n_particles"]
+        want = plain(s, *(c[o:o + n] for c in coords), arith)
+        o += n
+        for r in (rg, rp):
+            np.testing.assert_array_equal(r["steps"], want[4])
+            for k, w in zip(("x", "px", "y", "py"), want[:4]):
+                assert_bitwise(r[k], w, k)
+    assert res_graph[0]["steps"][7] == 0 and np.isnan(res_graph[0]["x"][7])
+
+
+def test_batch_graph_replays_identically(gpu):
+    sets, coords = sweep.heterogeneous_sets(seed=5, n_sets=6, n_range=(500, 4000),
+                                            turn_range=(200, 3000))
+    b = C.Batch(sets)
+    b.configure(C.ARITH_EXACT, 2, 128, 512)
+    b.load(*coords)
+    b.run(True)
+    first = [b.get(f) for f in (C.FIELD_X, C.FIELD_STEPS)]
+    b.run(True)
+    second = [b.get(f) for f in (C.FIELD_X, C.FIELD_STEPS)]
+    assert_bitwise(first[0], second[0])
+    np.testing.assert_array_equal(first[1], second[1])
+    max_turns = max(s["n_turns"] for s in sets)
+    done, length, chunks = 0, 128, 0
+    while done < max_turns:
+        done += min(length, max_turns - done)
+        length = min(2 * length, 512)
+        chunks += 1
+    assert b.n_chunks() == chunks
