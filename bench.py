@@ -275,7 +275,10 @@ def bench_adjoint(C):
             best = min(best, a.elapsed_time(b) * 1e-3)
         return best
 
-    t_adj = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100))
+    t_adj = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100,
+                                          reverse="inverse"))
+    t_replay = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100,
+                                             reverse="replay"))
     t_loss = timed(lambda: AG.per_particle(*pts, theta, nt, mode="loss"))
     tr = C.Tracker(nt, 0.168, 0.201, "sps", float("nan"), 16.0, 0)
     work = [torch.empty_like(p) for p in pts]
@@ -293,8 +296,9 @@ def bench_adjoint(C):
     t_track = timed(track)
     r = AG.per_particle(*pts, theta, nt, checkpoint_every=100)
     return {"workload": "65,536 particles, 1e4 turns, eps 16, mu 0.1, checkpoints every 100",
-            "adjoint_s": t_adj, "forward_track_s": t_track, "forward_loss_s": t_loss,
-            "adjoint_over_forward_track": t_adj / t_track,
+            "adjoint_s": t_adj, "adjoint_replay_s": t_replay, "forward_track_s": t_track,
+            "forward_loss_s": t_loss, "adjoint_over_forward_track": t_adj / t_track,
+            "reverse_sweep": "inverse map from the next checkpoint (replay variant also timed)",
             "survivors": int(r["survived"].sum().item()),
             "timing": "CUDA events, best of 3 after one warm-up"}
 

@@ -52,7 +52,7 @@ def _run(x0, px0, y0, py0, theta, n_turns, barrier, checkpoint_every, arith, mod
     g_ic = torch.empty((4, n), dtype=torch.float64, device=dev)
     g_th = torch.empty((4, n), dtype=torch.float64, device=dev)
     ws = None
-    if mode == 0:
+    if mode in (0, 3):
         nb = C.load().hm_adjoint_workspace_bytes(n, n_turns, checkpoint_every)
         ws = torch.empty(nb, dtype=torch.uint8, device=dev)
     torch.cuda.synchronize(dev)
@@ -68,10 +68,11 @@ class OrbitLoss(torch.autograd.Function):
     scales the stored gradients."""
 
     @staticmethod
-    def forward(ctx, x0, px0, y0, py0, theta, n_turns, barrier, checkpoint_every, arith, group):
+    def forward(ctx, x0, px0, y0, py0, theta, n_turns, barrier, checkpoint_every, arith, group,
+                reverse_mode):
         need = any(ctx.needs_input_grad[:5])
         loss, surv, _, g_ic, g_th = _run(x0, px0, y0, py0, theta, n_turns, barrier,
-                                         checkpoint_every, arith, 0 if need else 2)
+                                         checkpoint_every, arith, reverse_mode if need else 2)
         sums = torch.cat([loss.sum().reshape(1), surv.sum(dtype=torch.float64).reshape(1),
                           g_th.sum(dim=1) if need else torch.zeros(4, dtype=torch.float64,
                                                                     device=loss.device)])
@@ -89,30 +90,40 @@ class OrbitLoss(torch.autograd.Function):
         g_ic, g_th = ctx.saved_tensors
         s = grad_out / ctx.count
         gx, gpx, gy, gpy = (g_ic[k] * s for k in range(4))
-        return gx, gpx, gy, gpy, (g_th * grad_out).to(ctx.theta_device), None, None, None, None, None
+        return (gx, gpx, gy, gpy, (g_th * grad_out).to(ctx.theta_device), None, None, None, None,
+                None, None)
+
+
+# Reverse sweeps: "inverse" rebuilds each segment backwards with the map's
+# exact inverse from the next checkpoint (no scratch traffic); "replay"
+# recomputes it forward from its checkpoint into a scratch buffer (states
+# identical to the forward orbit).
+_REVERSE = {"inverse": 3, "replay": 0}
 
 
 def orbit_loss(x0, px0, y0, py0, theta, n_turns: int, barrier: float = 10.0,
-               checkpoint_every: int = 100, arith: str = "exact", group=None):
+               checkpoint_every: int = 100, arith: str = "exact", group=None,
+               reverse: str = "inverse"):
     """Mean Birkhoff-weighted orbit action over surviving particles (a 0-d
     tensor that backpropagates to x0..py0 and theta)."""
     mode = C.ARITH_FAST if arith == "fast" else C.ARITH_EXACT
     return OrbitLoss.apply(x0, px0, y0, py0, theta, int(n_turns), float(barrier),
-                           int(checkpoint_every), mode, group)
+                           int(checkpoint_every), mode, group, _REVERSE[reverse])
 
 
 def per_particle(x0, px0, y0, py0, theta, n_turns: int, barrier: float = 10.0,
-                 checkpoint_every: int = 100, arith: str = "exact", mode: str = "adjoint"):
+                 checkpoint_every: int = 100, arith: str = "exact", mode: str = "adjoint",
+                 reverse: str = "inverse"):
     """Per-particle values without autograd: dict with loss, survived, steps
     and (mode "adjoint") grad_ic [4, n], grad_theta [4, n] or (mode
     "tangent") grad_ic from forward-mode tangent-map propagation."""
-    m = {"adjoint": 0, "tangent": 1, "loss": 2}[mode]
+    m = {"adjoint": _REVERSE[reverse], "tangent": 1, "loss": 2}[mode]
     a = C.ARITH_FAST if arith == "fast" else C.ARITH_EXACT
     loss, surv, steps, g_ic, g_th = _run(x0, px0, y0, py0, theta, int(n_turns), float(barrier),
                                          int(checkpoint_every), a, m)
     out = {"loss": loss, "survived": surv.bool(), "steps": steps}
-    if m in (0, 1):
+    if m != 2:
         out["grad_ic"] = g_ic
-    if m == 0:
+    if m in (0, 3):
         out["grad_theta"] = g_th
     return out

@@ -32,17 +32,18 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, c
                      uint32_t *steps, double *grad_ic, double *grad_theta, void *workspace,
                      void *stream) {
     if (!t) return fail(HM_ERR_INVALID_ARG, "null tracker");
-    if (mode < 0 || mode > 2) return fail(HM_ERR_INVALID_ARG, "mode must be 0, 1 or 2");
+    if (mode < 0 || mode > 3) return fail(HM_ERR_INVALID_ARG, "mode must be 0, 1, 2 or 3");
     if (n_turns > t->allowed_steps) return fail(HM_ERR_BUDGET, "The number of turns is too large.");
     if (n == 0) return ok();
     if (!x0 || !px0 || !y0 || !py0 || !loss || !survived || !steps)
         return fail(HM_ERR_INVALID_ARG, "null device array");
-    if (mode == 0 && (checkpoint_every == 0 || !workspace || !grad_ic || !grad_theta))
+    const bool reverse = mode == 0 || mode == 3;
+    if (reverse && (checkpoint_every == 0 || !workspace || !grad_ic || !grad_theta))
         return fail(HM_ERR_INVALID_ARG, "the adjoint needs checkpoint_every > 0, a workspace and "
                                         "gradient outputs");
     if (mode == 1 && !grad_ic) return fail(HM_ERR_INVALID_ARG, "null gradient output");
     std::vector<double> ripple;
-    if (mode == 0) HM_TRY(hm::modulation_ripple(t->kind, n_turns, t->omega_0, t->offset, ripple));
+    if (reverse) HM_TRY(hm::modulation_ripple(t->kind, n_turns, t->omega_0, t->offset, ripple));
     DeviceBuffer dS, dw;
     HM_TRY(hm::upload(dS, ripple));
     HM_TRY(hm::upload(dw, hm::birkhoff_weights(n_turns)));
@@ -65,7 +66,7 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, c
     a.b2bits = 0;
     if (!std::isnan(b2)) std::memcpy(&a.b2bits, &b2, sizeof(b2));
     a.arith = t->arith;
-    if (mode == 0) {
+    if (reverse) {
         a.ckpt_buf = static_cast<double *>(workspace);
         a.seg_buf = a.ckpt_buf + ckpt_count(n_turns, checkpoint_every) * 4 * n;
     }

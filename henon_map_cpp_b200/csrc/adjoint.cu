@@ -178,6 +178,106 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const AdjointArgs a) {
     a.g_th[3 * n + i] = g_mu;
 }
 
+// Reverse sweep without a segment buffer: inside each segment the pre-turn
+// states are rebuilt backwards with the map's exact inverse (inverse
+// rotations, then the kicks subtracted), starting from the stored state at
+// the segment's end (the next checkpoint, or the final state).  Rounding
+// errors of the reconstruction can grow only across one segment, and the
+// per-turn memory traffic of the replay variant disappears.
+template <int ARITH, bool OCT>
+__global__ void __launch_bounds__(128) adjoint_inverse_kernel(const AdjointArgs a) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const size_t n = a.n;
+    const uint32_t N = a.n_turns, C = a.ckpt;
+    S4 s{a.x0[i], a.px0[i], a.y0[i], a.py0[i]};
+    bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
+    double loss = 0.0;
+    uint32_t k = 0;
+    for (; alive && k < N; ++k) {
+        if (k % C == 0) store4(a.ckpt_buf, k / C, n, i, s);
+        const double r = fwd<ARITH, OCT>(s, dev::load_turn(a.table, k), a.mu);
+        if (!inside(r, a.b2bits)) {
+            alive = false;
+            break;
+        }
+        loss = fma(a.w[k], r, loss);
+    }
+    a.steps[i] = alive ? N : k;
+    if (!alive) {
+        a.loss[i] = 0.0;
+        a.survived[i] = 0;
+        a.g_ic[i] = a.g_ic[n + i] = a.g_ic[2 * n + i] = a.g_ic[3 * n + i] = 0.0;
+        a.g_th[i] = a.g_th[n + i] = a.g_th[2 * n + i] = a.g_th[3 * n + i] = 0.0;
+        return;
+    }
+    a.loss[i] = loss;
+    a.survived[i] = 1;
+
+    const double mu = a.mu;
+    double lx = 0.0, lpx = 0.0, ly = 0.0, lpy = 0.0;
+    // sum_k gw_k and sum_k S_k gw_k per plane: the parameter gradients are
+    // combined from them at the end.
+    double Gx = 0.0, Gy = 0.0, Hx = 0.0, Hy = 0.0, g_mu = 0.0;
+    const S4 final_state = s;
+    const uint32_t n_seg = (N + C - 1) / C;
+    for (int seg = int(n_seg) - 1; seg >= 0; --seg) {
+        const uint32_t k0 = uint32_t(seg) * C;
+        const uint32_t k1 = min(k0 + C, N);
+        S4 post = (uint32_t(seg) + 1 < n_seg) ? load4(a.ckpt_buf, uint32_t(seg) + 1, n, i) : final_state;
+        for (uint32_t kk = k1; kk-- > k0;) {
+            const dev::Turn t = dev::load_turn(a.table, kk);
+            const double X = post.x, PX = post.px, Y = post.y, PY = post.py;
+            // inverse turn (henon_step reverse order, src/henon.cu:510-528)
+            const double x = fma(t.cx, X, -t.sx * PX), px1 = fma(t.sx, X, t.cx * PX);
+            const double y = fma(t.cy, Y, -t.sy * PY), py1 = fma(t.sy, Y, t.cy * PY);
+            const double xx = x * x, yy = y * y;
+            const double dxy = xx - yy;
+            const double ax3 = fma(-3.0, yy, xx), ay3 = fma(-3.0, xx, yy);
+            double qx = dxy, qy = -2.0 * x * y;
+            if (OCT) {
+                qx = fma(mu * x, ax3, qx);
+                qy = fma(mu * y, ay3, qy);
+            }
+            post = S4{x, px1 - qx, y, py1 - qy};
+            // adjoint of the post-turn state: lambda + w_k grad A
+            const double w2 = 2.0 * a.w[kk];
+            const double aX = fma(w2, X, lx), aPX = fma(w2, PX, lpx);
+            const double aY = fma(w2, Y, ly), aPY = fma(w2, PY, lpy);
+            const double gwx = fma(aX, PX, -aPX * X);
+            const double gwy = fma(aY, PY, -aPY * Y);
+            const double Sk = a.S[kk];
+            Gx += gwx;
+            Gy += gwy;
+            Hx = fma(Sk, gwx, Hx);
+            Hy = fma(Sk, gwy, Hy);
+            const double rx = fma(t.cx, aX, -t.sx * aPX), rpx = fma(t.sx, aX, t.cx * aPX);
+            const double ry = fma(t.cy, aY, -t.sy * aPY), rpy = fma(t.sy, aY, t.cy * aPY);
+            double da = 2.0 * x, db = -2.0 * y, dd = -2.0 * x;
+            if (OCT) {
+                da = fma(3.0 * mu, dxy, da);
+                db = fma(-6.0 * mu * x, y, db);
+                dd = fma(-3.0 * mu, dxy, dd);
+            }
+            // d(px1, py1)/d mu = (x (x^2 - 3y^2), y (y^2 - 3x^2)), also at mu = 0
+            g_mu = fma(rpx, x * ax3, fma(rpy, y * ay3, g_mu));
+            lx = fma(rpx, da, fma(rpy, db, rx));
+            ly = fma(rpx, db, fma(rpy, dd, ry));
+            lpx = rpx;
+            lpy = rpy;
+        }
+    }
+    a.g_ic[i] = lx;
+    a.g_ic[n + i] = lpx;
+    a.g_ic[2 * n + i] = ly;
+    a.g_ic[3 * n + i] = lpy;
+    // omega(k) = omega0 (1 + eps S_k): d/d omega0 = 1 + eps S_k, d/d eps = omega0 S_k
+    a.g_th[i] = fma(a.epsilon, Hx, Gx);
+    a.g_th[n + i] = fma(a.epsilon, Hy, Gy);
+    a.g_th[2 * n + i] = fma(a.omega_x0, Hx, a.omega_y0 * Hy);
+    a.g_th[3 * n + i] = g_mu;
+}
+
 // Forward mode: loss and, with TANGENT, g = sum_k w_k M_{k+1}^T grad A(x_{k+1})
 // with M_{k+1} = DF_k ... DF_0 (DF_k = tangent_matrix at x_k, table[k]).
 template <int ARITH, bool OCT, bool TANGENT>
@@ -238,6 +338,9 @@ cudaError_t launch_a(const AdjointArgs &a, int mode, cudaStream_t s) {
     if (mode == 0) {
         if (oct) adjoint_kernel<ARITH, true><<<blocks, 128, 0, s>>>(a);
         else adjoint_kernel<ARITH, false><<<blocks, 128, 0, s>>>(a);
+    } else if (mode == 3) {
+        if (oct) adjoint_inverse_kernel<ARITH, true><<<blocks, 128, 0, s>>>(a);
+        else adjoint_inverse_kernel<ARITH, false><<<blocks, 128, 0, s>>>(a);
     } else if (mode == 1) {
         if (oct) forward_loss_kernel<ARITH, true, true><<<blocks, 128, 0, s>>>(a);
         else forward_loss_kernel<ARITH, false, true><<<blocks, 128, 0, s>>>(a);

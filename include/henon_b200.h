@@ -407,8 +407,13 @@ hm_status hm_batch_get(const hm_batch *b, hm_field field, void *host_out);
  * dL_i/d(x0, px0, y0, py0) and grad_theta[4][n] = dL_i/d(omega_x0,
  * omega_y0, epsilon, mu), omega_{x,y}0 = 2 pi tune_{x,y}, with checkpoints
  * every checkpoint_every turns and recomputation in between (workspace of
- * hm_adjoint_workspace_bytes).  mode 1 gives grad_ic by forward-mode
- * tangent-map propagation (an independent J^T v), mode 2 the loss only.
+ * hm_adjoint_workspace_bytes).  mode 0 replays each segment from its
+ * checkpoint into the workspace (the states are the forward orbit's, bit
+ * for bit); mode 3 instead rebuilds them backwards with the map's exact
+ * inverse from the state at the segment's end (no per-turn memory traffic;
+ * reconstruction error bounded to one segment).  mode 1 gives grad_ic by
+ * forward-mode tangent-map propagation (an independent J^T v), mode 2 the
+ * loss only.
  * Derivatives need an "sps" or "basic" modulation.  Synchronous. */
 size_t hm_adjoint_workspace_bytes(size_t n, uint32_t n_turns,
                                   uint32_t checkpoint_every);
