@@ -28,7 +28,7 @@ except ImportError as _e:  # library not built: every class raises on use
 __all__ = ["gpu_available", "birkhoff_weights", "particles", "matrix_4d_vector", "vector_4d",
            "lyapunov_birkhoff_construct", "lyapunov_birkhoff_construct_multi",
            "megno_construct", "megno_birkhoff_construct", "tune_birkhoff_construct",
-           "henon_tracker", "storage_gpu"]
+           "henon_tracker", "storage", "storage_gpu"]
 
 
 def _engine():
@@ -320,6 +320,50 @@ class henon_tracker:
     def track(self, particles, n_turns, mu, barrier=10.0, kick_module=np.nan, inverse=False):
         self.tracker.track(particles.particles, n_turns, mu, barrier, kick_module, inverse)
 
+    def megno(self, particles, n_turns, mu, barrier=10.0, kick_module=np.nan, inverse=False,
+              turn_samples=np.array([]), n_threads=-1):
+        """MEGNO at turn_samples (default: n_turns), shape (n, samples).
+
+        Computed on the GPU with the megno_construct definition (Frobenius
+        norm of the tangent map of the orbit); the reference's CPU routine
+        uses the matrix trace instead and returns NaN in practice."""
+        return np.asarray(self.tracker.megno(particles.particles, n_turns, mu, barrier,
+                                             kick_module, inverse,
+                                             [int(s) for s in np.asarray(turn_samples).ravel()],
+                                             n_threads))
+
+    def tune_birkhoff(self, particles, n_turns, mu, barrier=10.0, kick_module=np.nan,
+                      inverse=False, from_idx=np.array([]), to_idx=np.array([])):
+        import pandas as pd
+
+        result = np.asarray(self.tracker.birkhoff_tunes(
+            particles.particles, n_turns, mu, barrier, kick_module, inverse,
+            [int(v) for v in np.asarray(from_idx).ravel()],
+            [int(v) for v in np.asarray(to_idx).ravel()]))
+        pd_result = pd.DataFrame(columns=["from", "to", "tune_x", "tune_y"])
+        for i in range(len(from_idx)):
+            pd_result.loc[i] = [from_idx[i], to_idx[i], result[:, i * 2], result[:, i * 2 + 1]]
+        pd_result.loc[len(from_idx)] = [0, n_turns, result[:, -2], result[:, -1]]
+        return pd_result
+
+    def tune_all(self, particles, n_turns, mu, barrier=10.0, kick_module=np.nan, inverse=False,
+                 from_idx=np.array([]), to_idx=np.array([])):
+        import pandas as pd
+
+        result_birkhoff, result_fft = (np.asarray(r) for r in self.tracker.all_tunes(
+            particles.particles, n_turns, mu, barrier, kick_module, inverse,
+            [int(v) for v in np.asarray(from_idx).ravel()],
+            [int(v) for v in np.asarray(to_idx).ravel()]))
+        pd_result = pd.DataFrame(columns=["from", "to", "tune_x_birkhoff", "tune_y_birkhoff",
+                                          "tune_x_fft", "tune_y_fft"])
+        for i in range(len(from_idx)):
+            pd_result.loc[i] = [from_idx[i], to_idx[i], result_birkhoff[:, i * 2],
+                                result_birkhoff[:, i * 2 + 1], result_fft[:, i * 2],
+                                result_fft[:, i * 2 + 1]]
+        pd_result.loc[len(from_idx)] = [0, n_turns, result_birkhoff[:, -2], result_birkhoff[:, -1],
+                                        result_fft[:, -2], result_fft[:, -1]]
+        return pd_result
+
     def get_tangent_matrix(self, particles, mu, reverse=False):
         return self.tracker.get_tangent_matrix(particles.particles, mu, reverse)
 
@@ -353,6 +397,54 @@ class henon_tracker:
             vectors=inner(vectors, "vector"), lyapunov=inner(lyapunov, "construct"),
             tune=inner(tune, "construct"),
             megno_sample_turns=[int(s) for s in megno_sample_turns]))
+
+
+class storage:
+    """Turn-by-turn snapshots kept on the host (storage_4d); the tune
+    estimates run on the GPU (hm_orbit_tunes)."""
+
+    def __init__(self, N):
+        self.N = N
+        self._x, self._px, self._y, self._py = [], [], [], []
+
+    def store(self, particles):
+        p = particles.particles
+        self._x.append(np.asarray(p.get_x())[:self.N])
+        self._px.append(np.asarray(p.get_px())[:self.N])
+        self._y.append(np.asarray(p.get_y())[:self.N])
+        self._py.append(np.asarray(p.get_py())[:self.N])
+
+    def _tunes(self, from_idx, to_idx, method):
+        return np.asarray(_engine().orbit_tunes(
+            np.asarray(self._x), np.asarray(self._px), np.asarray(self._y),
+            np.asarray(self._py), [int(v) for v in from_idx], [int(v) for v in to_idx], method))
+
+    def _frame(self, result, from_idx, to_idx, max_value):
+        import pandas as pd
+
+        pd_result = pd.DataFrame(columns=["from", "to", "tune_x", "tune_y"])
+        for i in range(len(from_idx)):
+            pd_result.loc[i] = [from_idx[i], to_idx[i], result[:, i * 2], result[:, i * 2 + 1]]
+        pd_result.loc[len(from_idx)] = [0, max_value, result[:, -2], result[:, -1]]
+        return pd_result
+
+    def tune_fft(self, from_idx, to_idx, max_value):
+        return self._frame(self._tunes(from_idx, to_idx, 1), from_idx, to_idx, max_value)
+
+    def tune_birkhoff(self, from_idx, to_idx, max_value):
+        return self._frame(self._tunes(from_idx, to_idx, 0), from_idx, to_idx, max_value)
+
+    def get_x(self):
+        return np.asarray(self._x).T
+
+    def get_px(self):
+        return np.asarray(self._px).T
+
+    def get_y(self):
+        return np.asarray(self._y).T
+
+    def get_py(self):
+        return np.asarray(self._py).T
 
 
 class storage_gpu:

@@ -163,6 +163,14 @@ _SIGNATURES = {
     "hm_batch_load": (None, [c_void_p, _PD, _PD, _PD, _PD]),
     "hm_batch_run": (None, [c_void_p, c_int]),
     "hm_batch_get": (None, [c_void_p, c_int, c_void_p]),
+    # tunes
+    "hm_orbit_tunes": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t,
+                              _PU32, _PU32, c_size_t, c_int, _PD]),
+    "hm_tracker_orbit_tunes": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, _PU32,
+                                      _PU32, c_size_t, c_int, _PD, _PD]),
+    "hm_storage_tunes": (None, [c_void_p, _PU32, _PU32, c_size_t, c_int, _PD]),
+    "hm_orbit_tunes_host": (None, [_PD, _PD, _PD, _PD, c_size_t, c_size_t, _PU32, _PU32,
+                                   c_size_t, c_int, _PD]),
     # orbit-loss gradients
     "hm_adjoint_workspace_bytes": (c_size_t, [c_size_t, c_uint32, c_uint32]),
     "hm_adjoint": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_double,
@@ -184,7 +192,8 @@ class IndicatorSet(ctypes.Structure):
     _fields_ = [("matrix", c_void_p), ("matrix_old", c_void_p), ("megno", c_void_p),
                 ("megno_birkhoff", c_void_p), ("vectors", c_void_p), ("lyapunov", c_void_p),
                 ("tune", c_void_p), ("megno_sample_turns", POINTER(c_uint64)),
-                ("n_megno_samples", c_size_t), ("megno_samples_out", _PD)]
+                ("n_megno_samples", c_size_t), ("megno_samples_out", _PD),
+                ("jacobian_of_turn", c_int)]
 
 _lib: ctypes.CDLL | None = None
 
@@ -554,9 +563,11 @@ class Storage(_Handle):
 def track_indicators(tracker: Tracker, particles: Particles, n_turns: int, mu: float,
                      barrier: float = 100.0, matrix=None, matrix_old=None, megno=None,
                      megno_birkhoff=None, vectors=None, lyapunov=None, tune=None,
-                     megno_sample_turns=None, megno_samples_out=None):
+                     megno_sample_turns=None, megno_samples_out=None,
+                     jacobian_of_turn=False):
     """hm_track_indicators: n_turns of the fused per-turn indicator loop."""
     s = IndicatorSet()
+    s.jacobian_of_turn = int(bool(jacobian_of_turn))
     for name, obj in (("matrix", matrix), ("matrix_old", matrix_old), ("megno", megno),
                       ("megno_birkhoff", megno_birkhoff), ("vectors", vectors),
                       ("lyapunov", lyapunov), ("tune", tune)):
@@ -618,6 +629,35 @@ class Batch(_Handle):
         out = np.empty(self.n_total, dtype=FIELD_DTYPE[field])
         call("hm_batch_get", self.h, int(field), out.ctypes.data_as(c_void_p))
         return out
+
+
+def _windows(frm, to):
+    f = np.ascontiguousarray(np.asarray(frm, dtype=np.uint32).ravel())
+    t = np.ascontiguousarray(np.asarray(to, dtype=np.uint32).ravel())
+    if f.size != t.size:
+        raise ValueError("compute_tune: from and to must be of the same size")
+    return f, t
+
+
+def tracker_orbit_tunes(tracker: Tracker, particles: Particles, n_turns: int, mu: float,
+                        barrier: float, frm, to, remove_mean: bool, fft: bool):
+    """hm_tracker_orbit_tunes: (birkhoff [n][2(W+1)], fft or None)."""
+    f, t = _windows(frm, to)
+    n = particles.n_total
+    b = np.empty((n, 2 * (f.size + 1)))
+    ff = np.empty_like(b) if fft else None
+    call("hm_tracker_orbit_tunes", tracker.h, particles.h, int(n_turns), float(mu),
+         float(barrier), f.ctypes.data_as(_PU32), t.ctypes.data_as(_PU32), f.size,
+         int(bool(remove_mean)), dptr(b), dptr(ff) if fft else None)
+    return b, ff
+
+
+def storage_tunes(storage: "Storage", frm, to, method: int) -> np.ndarray:
+    f, t = _windows(frm, to)
+    out = np.empty((storage.n, 2 * (f.size + 1)))
+    call("hm_storage_tunes", storage.h, f.ctypes.data_as(_PU32), t.ctypes.data_as(_PU32), f.size,
+         int(method), dptr(out))
+    return out
 
 
 def set_track_config(threads: int, per_thread: int, chunk0: int, chunk_max: int) -> None:

@@ -36,9 +36,9 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
              f"-I{CUDA_HOME / 'include'}", f"-I{INCLUDE}"]
 
 CU_SOURCES = ["track.cu", "noalloc.cu", "tangent.cu", "fused.cu", "ghosts.cu", "batch.cu",
-              "adjoint.cu"]
+              "adjoint.cu", "tunes.cu"]
 CPP_SOURCES = ["capi.cpp", "modulation.cpp", "indicators.cpp", "particles_extra.cpp",
-               "batch.cpp", "adjoint.cpp"]
+               "batch.cpp", "adjoint.cpp", "tunes.cpp"]
 
 
 def _run(cmd: list[str]) -> None:
@@ -75,7 +75,7 @@ def build_library(force: bool = False) -> Path:
         objs.append(o)
     if force or _stale(LIB, objs):
         _run([NVCC, "-shared", *ARCH, "-o", str(LIB), *map(str, objs),
-              "-lcudart", "-lpthread"])
+              "-lcudart", "-lcufft", "-lpthread"])
     return LIB
 
 

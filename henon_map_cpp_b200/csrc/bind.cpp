@@ -1,5 +1,5 @@
 // pybind11 module `henon_map_engine`: the reference's Python-facing engine
-// (src/bind.cpp:224-578) re-exposed over the C ABI of libhenon_b200.so.
+// (src/bind.cpp:224-577) re-exposed over the C ABI of libhenon_b200.so.
 //
 // Class names, method names, argument names and defaults follow the
 // reference's GPU classes (particles_4d_gpu, henon_tracker_gpu,
@@ -288,6 +288,23 @@ PYBIND11_MODULE(henon_map_engine, m) {
                             other.data()));
         return out;
     }, py::arg("from"), py::arg("to"), py::arg("start"), py::arg("end"));
+    m.def("orbit_tunes", [](py::array_t<double, py::array::c_style | py::array::forcecast> x,
+                            py::array_t<double, py::array::c_style | py::array::forcecast> px,
+                            py::array_t<double, py::array::c_style | py::array::forcecast> y,
+                            py::array_t<double, py::array::c_style | py::array::forcecast> py_,
+                            std::vector<uint32_t> from, std::vector<uint32_t> to, int method) {
+        // Tunes of host orbits [samples][particles]: windows + full orbit.
+        if (x.ndim() != 2 || px.ndim() != 2 || y.ndim() != 2 || py_.ndim() != 2)
+            throw py::value_error("orbits must be 2D [samples][particles]");
+        const size_t S = size_t(x.shape(0)), n = size_t(x.shape(1));
+        if (from.size() != to.size())
+            throw std::runtime_error("compute_tune: from and to must be of the same size");
+        auto out = array2(n, 2 * (from.size() + 1));
+        check(hm_orbit_tunes_host(x.data(), px.data(), y.data(), py_.data(), n, S, from.data(),
+                                  to.data(), from.size(), method, out.mutable_data()));
+        return out;
+    }, py::arg("x"), py::arg("px"), py::arg("y"), py::arg("py"), py::arg("from_idx"),
+       py::arg("to_idx"), py::arg("method"));
     m.def("birkhoff_weights", [](unsigned n) {
         auto out = array1<double>(n);
         check(hm_birkhoff_weights(n, out.mutable_data()));
@@ -392,6 +409,88 @@ PYBIND11_MODULE(henon_map_engine, m) {
             check(hm_tracker_allowed_steps(t.h, &n));
             return n;
         })
+        .def("birkhoff_tunes", [](Tracker &t, Particles &p, unsigned n_turns, double mu,
+                                  double barrier, double kick, bool inverse,
+                                  std::vector<uint32_t> from, std::vector<uint32_t> to) {
+            // henon_tracker::birkhoff_tunes (src/henon.cu:2890-2967): the
+            // window [0, n_turns] is appended to the caller's, then the full
+            // orbit; result [n][2 (W + 2)].
+            if (!std::isnan(kick) || inverse)
+                throw std::domain_error("birkhoff_tunes: kicks and inverse tracking are not provided");
+            if (from.size() != to.size())
+                throw std::runtime_error("compute_tune: from and to must be of the same size");
+            from.push_back(0);
+            to.push_back(n_turns);
+            auto out = array2(p.n_total(), 2 * (from.size() + 1));
+            hm_status s;
+            {
+                py::gil_scoped_release nogil;
+                s = hm_tracker_orbit_tunes(t.h, p.h, n_turns, mu, barrier, from.data(), to.data(),
+                                           from.size(), 0, out.mutable_data(), nullptr);
+            }
+            check(s);
+            return out;
+        }, py::arg("particles"), py::arg("n_turns"), py::arg("mu"), py::arg("barrier") = 100.0,
+           py::arg("kick_module") = NAN, py::arg("inverse") = false,
+           py::arg("from_idx") = std::vector<uint32_t>(), py::arg("to_idx") = std::vector<uint32_t>())
+        .def("all_tunes", [](Tracker &t, Particles &p, unsigned n_turns, double mu,
+                             double barrier, double kick, bool inverse, std::vector<uint32_t> from,
+                             std::vector<uint32_t> to) {
+            // henon_tracker::all_tunes (src/henon.cu:2969-3078): orbit mean
+            // removed, Birkhoff and FFT tunes; ([n][2(W+2)], [n][2(W+2)]).
+            if (!std::isnan(kick) || inverse)
+                throw std::domain_error("all_tunes: kicks and inverse tracking are not provided");
+            if (from.size() != to.size())
+                throw std::runtime_error("compute_tune: from and to must be of the same size");
+            from.push_back(0);
+            to.push_back(n_turns);
+            auto b = array2(p.n_total(), 2 * (from.size() + 1));
+            auto f = array2(p.n_total(), 2 * (from.size() + 1));
+            hm_status s;
+            {
+                py::gil_scoped_release nogil;
+                s = hm_tracker_orbit_tunes(t.h, p.h, n_turns, mu, barrier, from.data(), to.data(),
+                                           from.size(), 1, b.mutable_data(), f.mutable_data());
+            }
+            check(s);
+            return py::make_tuple(b, f);
+        }, py::arg("particles"), py::arg("n_turns"), py::arg("mu"), py::arg("barrier") = 100.0,
+           py::arg("kick_module") = NAN, py::arg("inverse") = false,
+           py::arg("from_idx") = std::vector<uint32_t>(), py::arg("to_idx") = std::vector<uint32_t>())
+        .def("megno", [](Tracker &t, Particles &p, unsigned n_turns, double mu, double barrier,
+                         double kick, bool inverse, std::vector<uint64_t> samples, int) {
+            // Whole-orbit MEGNO (henon_tracker::megno, src/henon.cu:2755-2887)
+            // with the GPU construct's definition (Frobenius norm of the
+            // tangent map, src/henon.cu:2253-2284) and the tangent map of each
+            // turn; values at the turn counts in turn_samples: [n][samples].
+            if (!std::isnan(kick) || inverse)
+                throw std::domain_error("megno: kicks and inverse tracking are not provided");
+            if (samples.empty()) samples.push_back(n_turns);
+            const size_t n = p.n_total();
+            Matrices M(n);
+            Megno g(n);
+            std::vector<double> snap(samples.size() * n, std::numeric_limits<double>::quiet_NaN());
+            hm_indicator_set s{};
+            s.matrix = M.h;
+            s.megno = g.h;
+            s.megno_sample_turns = samples.data();
+            s.n_megno_samples = samples.size();
+            s.megno_samples_out = snap.data();
+            s.jacobian_of_turn = 1;
+            hm_status st;
+            {
+                py::gil_scoped_release nogil;
+                st = hm_track_indicators(t.h, p.h, n_turns, mu, barrier, &s);
+            }
+            check(st);
+            auto out = array2(n, samples.size());
+            double *o = out.mutable_data();
+            for (size_t i = 0; i < n; ++i)
+                for (size_t j = 0; j < samples.size(); ++j) o[i * samples.size() + j] = snap[j * n + i];
+            return out;
+        }, py::arg("particles"), py::arg("n_turns"), py::arg("mu"), py::arg("barrier") = 100.0,
+           py::arg("kick_module") = NAN, py::arg("inverse") = false,
+           py::arg("turn_samples") = std::vector<uint64_t>(), py::arg("n_threads") = -1)
         .def("track_indicators", [](Tracker &t, Particles &p, unsigned n_turns, double mu,
                                     double barrier, Matrices *matrix, Matrices *matrix_old,
                                     Megno *megno, MegnoBirkhoff *megno_b, Vectors *vectors,
@@ -548,5 +647,19 @@ PYBIND11_MODULE(henon_map_engine, m) {
         .def("get_x", [](const Storage &s) { return s.get(HM_FIELD_X); })
         .def("get_px", [](const Storage &s) { return s.get(HM_FIELD_PX); })
         .def("get_y", [](const Storage &s) { return s.get(HM_FIELD_Y); })
-        .def("get_py", [](const Storage &s) { return s.get(HM_FIELD_PY); });
+        .def("get_py", [](const Storage &s) { return s.get(HM_FIELD_PY); })
+        .def("tune_birkhoff", [](const Storage &s, std::vector<uint32_t> from, std::vector<uint32_t> to) {
+            if (from.size() != to.size())
+                throw std::runtime_error("compute_tune: from and to must be of the same size");
+            auto out = array2(s.n, 2 * (from.size() + 1));
+            check(hm_storage_tunes(s.h, from.data(), to.data(), from.size(), 0, out.mutable_data()));
+            return out;
+        }, py::arg("from_idx"), py::arg("to_idx"))
+        .def("tune_fft", [](const Storage &s, std::vector<uint32_t> from, std::vector<uint32_t> to) {
+            if (from.size() != to.size())
+                throw std::runtime_error("compute_tune: from and to must be of the same size");
+            auto out = array2(s.n, 2 * (from.size() + 1));
+            check(hm_storage_tunes(s.h, from.data(), to.data(), from.size(), 1, out.mutable_data()));
+            return out;
+        }, py::arg("from_idx"), py::arg("to_idx"));
 }

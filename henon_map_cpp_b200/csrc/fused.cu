@@ -120,6 +120,12 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     bool warp_live = __any_sync(dev::kFullMask, alive);
     uint32_t k = 0;
     for (; k < a.n_turns && warp_live; ++k) {
+        double df[16];
+        // ---- Jacobian of the turn, at the point before it (option) ------------
+        if ((DO_M || DO_V) && a.df_before) {
+            const dev::Turn td = dev::load_turn(a.table, a.live_step + k);
+            dev::tangent_matrix_exact(x, y, td, mu, df);
+        }
         // ---- track(p, 1) ------------------------------------------------------
         if (alive) {
             const dev::Turn t = dev::load_turn(a.table, a.live_step + k);
@@ -132,8 +138,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
             }
         }
         // ---- tangent matrix at the new point, table[global_steps] -------------
-        double df[16];
-        if (DO_M || DO_V) {
+        if ((DO_M || DO_V) && !a.df_before) {
             const dev::Turn td = dev::load_turn(a.table, a.global_step + k + 1u);
             dev::tangent_matrix_exact(x, y, td, mu, df);
         }

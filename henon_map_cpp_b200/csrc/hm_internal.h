@@ -212,6 +212,7 @@ struct FusedArgs {
     uint32_t n_turns;
     double mu;
     long long b2bits;
+    int df_before;  // 1: DF at the point before the turn, table[live_step + k]
     // tangent matrix and MEGNO
     double *M;
     double *megno_l1, *megno_l2, *megno_l3;
@@ -311,6 +312,33 @@ struct AdjointArgs {
 // mode 0: loss + reverse-mode gradients; 1: loss + forward-mode initial-
 // condition gradient (tangent map); 2: loss only.
 cudaError_t launch_adjoint(const AdjointArgs &a, int mode, cudaStream_t s);
+
+// ---- orbit tunes (tunes.cu / tunes.cpp) -----------------------------------------
+
+struct OrbitRecordArgs {
+    double *x, *px, *y, *py;  // particle state (updated)
+    uint32_t *steps;
+    size_t n;
+    const double *table;
+    uint32_t live_step, n_turns;
+    double mu;
+    long long b2bits;
+    int arith;
+    double *ox, *opx, *oy, *opy;  // orbit [n_turns + 1][n]
+};
+
+cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s);
+cudaError_t launch_mean_remove(double *x, double *px, double *y, double *py, size_t n, size_t S,
+                               cudaStream_t s);
+cudaError_t launch_birkhoff_tunes(const double *x, const double *px, const double *y,
+                                  const double *py, size_t n, const uint32_t *from,
+                                  const uint32_t *to, const uint64_t *w_off, const double *w,
+                                  int n_win, double *out, cudaStream_t s);
+cudaError_t launch_hann_gather(const double *q, const double *p, size_t n, uint32_t from,
+                               uint32_t len, size_t first, size_t count, double2 *buf,
+                               int *nan_flags, cudaStream_t s);
+cudaError_t launch_fft_peak(const double2 *buf, uint32_t len, size_t count, const int *nan_flags,
+                            double *out, size_t out_stride, size_t first, cudaStream_t s);
 
 // (Re)allocates and uploads the device arrays of p (capi.cpp).
 hm_status particles_upload(hm_particles *p, const double *x, const double *px, const double *y,

@@ -596,7 +596,7 @@ hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, 
                                         "n_megno_birkhoff + 2 n_lyapunov + 4 n_tune = 96)");
     // Turn budget (src/henon.cu:3158-3167) and the table read of
     // structured_multiply after the last turn.
-    const bool tangent = s.matrix || s.vectors;
+    const bool tangent = (s.matrix || s.vectors) && !s.jacobian_of_turn;
     if (uint64_t(n_turns) + p->global_steps + (tangent ? 1 : 0) > t->allowed_steps)
         return fail(HM_ERR_BUDGET, "The number of turns is too large.");
     if (n_turns == 0) return ok();
@@ -626,6 +626,7 @@ hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, 
     const double b2 = barrier * barrier;
     a.b2bits = 0;
     if (!std::isnan(b2)) std::memcpy(&a.b2bits, &b2, sizeof(b2));
+    a.df_before = s.jacobian_of_turn ? 1 : 0;
     if (s.matrix) a.M = s.matrix->m.as<double>();
     if (s.megno) {
         a.megno_l1 = s.megno->l1.as<double>();

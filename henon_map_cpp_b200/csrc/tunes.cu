@@ -1,0 +1,307 @@
+// Tune estimates from turn-by-turn orbits (sm_100a).
+//
+// An orbit buffer holds S snapshots of n particles per coordinate, laid
+// out [sample][particle] (storage_4d_gpu's layout), so a warp reads 32
+// particles of one sample in one coalesced access.
+//
+// * orbit_record_kernel: tracks n_turns turns and writes every state
+//   (sample 0 = the start), like the reference's CPU tune routines that
+//   store the orbit before computing tunes (src/henon.cu:2890-3078);
+// * mean_remove_kernel: subtracts each coordinate's orbit mean
+//   (src/henon.cu:3040-3051);
+// * birkhoff_kernel: Birkhoff-weighted phase advance over sample windows
+//   (birkhoff_tune / birkhoff_tune_vec, src/dynamic_indicator.cpp:81-131,
+//   198-253);
+// * hann_gather_kernel + cuFFT + fft_peak_kernel: Hann-windowed spectrum of
+//   x + i px and the interpolated peak (compute_fft, interpolation, A,
+//   fft_tune_vec, src/dynamic_indicator.cpp:32-61, 134-196, 255-330).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hm_device.cuh"
+#include "hm_internal.h"
+
+namespace hm {
+namespace {
+
+using dev::Rn;
+
+__device__ __forceinline__ bool inside(double r, long long b2bits) {
+    return static_cast<unsigned long long>(__double_as_longlong(r)) <
+           static_cast<unsigned long long>(b2bits);
+}
+
+template <int ARITH, bool OCT>
+__device__ __forceinline__ double map_turn(double &x, double &px, double &y, double &py,
+                                           const dev::Turn &t, double mu) {
+    if (ARITH == HM_ARITH_EXACT) {
+        const double xx = Rn::mul(x, x), yy = Rn::mul(y, y);
+        double npx = Rn::add(px, Rn::sub(xx, yy));
+        double npy = Rn::add(py, Rn::mul(Rn::mul(-2.0, x), y));
+        if (OCT) {
+            npx = Rn::add(npx, Rn::mul(mu, Rn::sub(Rn::mul(xx, x), Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
+            npy = Rn::add(npy, Rn::mul(mu, Rn::sub(Rn::mul(yy, y), Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
+        }
+        const double nx = Rn::add(Rn::mul(x, t.cx), Rn::mul(npx, t.sx));
+        npx = Rn::add(Rn::mul(-x, t.sx), Rn::mul(npx, t.cx));
+        const double ny = Rn::add(Rn::mul(y, t.cy), Rn::mul(npy, t.sy));
+        npy = Rn::add(Rn::mul(-y, t.sy), Rn::mul(npy, t.cy));
+        x = nx;
+        px = npx;
+        y = ny;
+        py = npy;
+        return Rn::add(Rn::add(Rn::mul(x, x), Rn::mul(px, px)), Rn::add(Rn::mul(y, y), Rn::mul(py, py)));
+    }
+    const double xx = x * x, yy = y * y;
+    double npx = px + (xx - yy);
+    double npy = fma(-2.0 * x, y, py);
+    if (OCT) {
+        npx = fma(mu * x, fma(-3.0, yy, xx), npx);
+        npy = fma(mu * y, fma(-3.0, xx, yy), npy);
+    }
+    const double nx = fma(x, t.cx, npx * t.sx);
+    npx = fma(npx, t.cx, -x * t.sx);
+    const double ny = fma(y, t.cy, npy * t.sy);
+    npy = fma(npy, t.cy, -y * t.sy);
+    x = nx;
+    px = npx;
+    y = ny;
+    py = npy;
+    return fma(px, px, x * x) + fma(py, py, y * y);
+}
+
+template <int ARITH, bool OCT>
+__global__ void orbit_record_kernel(OrbitRecordArgs a) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const size_t n = a.n;
+    double x = a.x[i], px = a.px[i], y = a.y[i], py = a.py[i];
+    uint32_t steps = a.steps[i];
+    bool alive = !dev::is_lost(x, px, y, py);
+    a.ox[i] = x;
+    a.opx[i] = px;
+    a.oy[i] = y;
+    a.opy[i] = py;
+    for (uint32_t k = 0; k < a.n_turns; ++k) {
+        if (alive) {
+            const double r = map_turn<ARITH, OCT>(x, px, y, py, dev::load_turn(a.table, a.live_step + k), a.mu);
+            if (inside(r, a.b2bits)) {
+                steps += 1u;
+            } else {
+                x = px = y = py = dev::quiet_nan();
+                alive = false;
+            }
+        }
+        const size_t o = size_t(k + 1) * n + i;
+        a.ox[o] = x;
+        a.opx[o] = px;
+        a.oy[o] = y;
+        a.opy[o] = py;
+    }
+    a.x[i] = x;
+    a.px[i] = px;
+    a.y[i] = y;
+    a.py[i] = py;
+    a.steps[i] = steps;
+}
+
+// v -= mean(v) per particle and coordinate; the mean is the left-to-right
+// sum from 0.0 divided by the sample count (std::accumulate / size).
+__global__ void mean_remove_kernel(double *x, double *px, double *y, double *py, size_t n,
+                                   size_t S) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *c[4] = {x, px, y, py};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double s = 0.0;
+        for (size_t k = 0; k < S; ++k) s = Rn::add(s, c[q][k * n + i]);
+        const double m = Rn::div(s, double(S));
+        for (size_t k = 0; k < S; ++k) c[q][k * n + i] = Rn::sub(c[q][k * n + i], m);
+    }
+}
+
+// Birkhoff tune over samples [from, to] of (q, p): 1 - sum_i w_i dtheta_i /
+// (2 pi), dtheta wrapped by +2pi when negative, w = birkhoff_weights(to -
+// from); NaN when check_nan and any sample of the window is NaN.
+__device__ double birkhoff_window(const double *q, const double *p, size_t n, size_t i,
+                                  uint32_t from, uint32_t to, const double *w, bool check_nan,
+                                  bool *has_nan) {
+    double sum = 0.0;
+    bool nan_seen = false;
+    double prev = atan2(p[size_t(from) * n + i], q[size_t(from) * n + i]);
+    nan_seen |= isnan(q[size_t(from) * n + i]) || isnan(p[size_t(from) * n + i]);
+    for (uint32_t s = from; s < to; ++s) {
+        const double qq = q[size_t(s + 1) * n + i], pp = p[size_t(s + 1) * n + i];
+        nan_seen |= isnan(qq) || isnan(pp);
+        const double th = atan2(pp, qq);
+        double d = Rn::sub(th, prev);
+        if (d < 0.0) d = Rn::add(d, 2.0 * M_PI);
+        sum = Rn::add(sum, Rn::mul(w[s - from], d));
+        prev = th;
+    }
+    *has_nan = nan_seen;
+    (void)check_nan;
+    return Rn::sub(1.0, Rn::div(sum, Rn::mul(2.0, M_PI)));
+}
+
+__global__ void birkhoff_kernel(const double *x, const double *px, const double *y,
+                                const double *py, size_t n, const uint32_t *from,
+                                const uint32_t *to, const uint64_t *w_off, const double *w,
+                                int n_win, double *out) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cols = 2 * n_win;
+    for (int j = 0; j < n_win; ++j) {
+        bool nx = false, ny = false;
+        double tx = birkhoff_window(x, px, n, i, from[j], to[j], w + w_off[j], true, &nx);
+        double ty = birkhoff_window(y, py, n, i, from[j], to[j], w + w_off[j], true, &ny);
+        // birkhoff_tune_vec checks all four coordinates of the window for
+        // the windows it was given, not for the appended full orbit.
+        const bool is_full = j == n_win - 1;
+        if (!is_full && (nx || ny)) tx = ty = dev::quiet_nan();
+        out[i * cols + 2 * j] = tx;
+        out[i * cols + 2 * j + 1] = ty;
+    }
+}
+
+// z_k = (x + i px)[from + k] * 2 sin^2(pi k / len) for one window, one row
+// of len complex values per particle; nan_flags[i] set when any sample of
+// the window is NaN.
+__global__ void hann_gather_kernel(const double *q, const double *p, size_t n, uint32_t from,
+                                   uint32_t len, size_t first, size_t count, double2 *buf,
+                                   int *nan_flags) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= count * len) return;
+    const size_t r = t / len, k = t % len;
+    const size_t i = first + r;
+    const double re = q[size_t(from + k) * n + i], im = p[size_t(from + k) * n + i];
+    if (isnan(re) || isnan(im)) nan_flags[r] = 1;
+    const double s = sin(M_PI * double(k) / double(len));
+    const double h = 2 * pow(s, 2);
+    buf[r * len + k] = make_double2(re * h, im * h);
+}
+
+// A(a, b, c) of the peak interpolation (src/dynamic_indicator.cpp:134-137).
+__device__ double interp_a(double a, double b, double c) {
+    return (-(a + b * c) * (a - b) +
+            b * sqrt(pow(c, 2) * pow((a + b), 2) - 2 * a * b * (2 * pow(c, 2) - c - 1))) /
+           (pow(a, 2) + pow(b, 2) + 2 * a * b * c);
+}
+
+// One warp per particle: argmax of |FFT| (first maximum), then the
+// interpolation of src/dynamic_indicator.cpp:139-176 -> |1 - value|.
+__global__ void fft_peak_kernel(const double2 *buf, uint32_t len, size_t count,
+                                const int *nan_flags, double *out, size_t out_stride,
+                                size_t first) {
+    const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const unsigned lane = threadIdx.x & 31u;
+    if (warp >= count) return;
+    const double2 *row = buf + warp * len;
+    double best = -1.0;
+    uint32_t best_k = 0xffffffffu;
+    for (uint32_t k = lane; k < len; k += 32) {
+        const double2 z = row[k];
+        const double m = sqrt(z.x * z.x + z.y * z.y);
+        if (m > best || (m == best && k < best_k)) {
+            best = m;
+            best_k = k;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(dev::kFullMask, best, o);
+        const uint32_t ok = __shfl_down_sync(dev::kFullMask, best_k, o);
+        if (ob > best || (ob == best && ok < best_k)) {
+            best = ob;
+            best_k = ok;
+        }
+    }
+    if (lane != 0) return;
+    double value;
+    if (nan_flags[warp]) {
+        value = dev::quiet_nan();
+    } else {
+        uint32_t index = best_k;
+        const double N = double(len);
+        auto mag = [&](uint32_t k) {
+            const double2 z = row[k];
+            return sqrt(z.x * z.x + z.y * z.y);
+        };
+        if (index == 0) {
+            value = 1.0;
+        } else if (index == len - 1) {
+            value = 0.0;
+        } else {
+            uint32_t i1, i2;
+            if (mag(index - 1) > mag(index + 1)) {
+                i1 = index - 1;
+                i2 = index;
+                index = index - 1;
+            } else {
+                i1 = index;
+                i2 = index + 1;
+            }
+            const double v = (double(index) / N) +
+                             (1.0 / (2.0 * M_PI)) *
+                                 asin(interp_a(mag(i1), mag(i2), cos(2.0 * M_PI / N)) *
+                                      sin(2.0 * M_PI / N));
+            value = fabs(1.0 - v);
+        }
+    }
+    out[(first + warp) * out_stride] = value;
+}
+
+}  // namespace
+
+cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    const unsigned blocks = unsigned((a.n + 127) / 128);
+    const bool oct = a.mu != 0.0;
+    if (a.arith == HM_ARITH_FAST) {
+        if (oct) orbit_record_kernel<HM_ARITH_FAST, true><<<blocks, 128, 0, s>>>(a);
+        else orbit_record_kernel<HM_ARITH_FAST, false><<<blocks, 128, 0, s>>>(a);
+    } else {
+        if (oct) orbit_record_kernel<HM_ARITH_EXACT, true><<<blocks, 128, 0, s>>>(a);
+        else orbit_record_kernel<HM_ARITH_EXACT, false><<<blocks, 128, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mean_remove(double *x, double *px, double *y, double *py, size_t n, size_t S,
+                               cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    mean_remove_kernel<<<unsigned((n + 127) / 128), 128, 0, s>>>(x, px, y, py, n, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_birkhoff_tunes(const double *x, const double *px, const double *y,
+                                  const double *py, size_t n, const uint32_t *from,
+                                  const uint32_t *to, const uint64_t *w_off, const double *w,
+                                  int n_win, double *out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    birkhoff_kernel<<<unsigned((n + 127) / 128), 128, 0, s>>>(x, px, y, py, n, from, to, w_off,
+                                                              w, n_win, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hann_gather(const double *q, const double *p, size_t n, uint32_t from,
+                               uint32_t len, size_t first, size_t count, double2 *buf,
+                               int *nan_flags, cudaStream_t s) {
+    const size_t total = count * len;
+    if (total == 0) return cudaSuccess;
+    hann_gather_kernel<<<unsigned((total + 255) / 256), 256, 0, s>>>(q, p, n, from, len, first,
+                                                                      count, buf, nan_flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_peak(const double2 *buf, uint32_t len, size_t count, const int *nan_flags,
+                            double *out, size_t out_stride, size_t first, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    const size_t threads = count * 32;
+    fft_peak_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(buf, len, count, nan_flags,
+                                                                    out, out_stride, first);
+    return cudaGetLastError();
+}
+
+}  // namespace hm

@@ -7,7 +7,7 @@
  * thread is available from hm_last_error().
  *
  * Reference interfaces replaced (paths inside carlidel/henon_map_cpp):
- *   - src/bind.cpp:224-578      pybind11 module `henon_map_engine`
+ *   - src/bind.cpp:224-577      pybind11 module `henon_map_engine`
  *   - src/henon.h:41-447        particles_4d[_gpu], henon_tracker[_gpu], the
  *                               tangent-map, indicator and storage classes
  *   - src/modulation.h:12-22    modulation tables
@@ -351,6 +351,11 @@ typedef struct hm_indicator_set {
     const uint64_t *megno_sample_turns;
     size_t n_megno_samples;
     double *megno_samples_out; /* host double[n_megno_samples][n] or NULL */
+    /* 0: the loop above (DF of the new point with table[global_steps], as
+     * structured_multiply after track); 1: DF of the turn itself, at the
+     * point before the turn with table[steps] (the tangent map of the
+     * orbit; needs no extra table entry). */
+    int jacobian_of_turn;
 } hm_indicator_set;
 
 hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns,
@@ -394,6 +399,46 @@ hm_status hm_batch_load(hm_batch *b, const double *x, const double *px,
 hm_status hm_batch_run(hm_batch *b, int use_graph);
 /* Host copy of x, px, y, py (double) or steps (uint32), concatenated. */
 hm_status hm_batch_get(const hm_batch *b, hm_field field, void *host_out);
+
+/* ---- tunes from turn-by-turn orbits ---------------------------------------
+ * An orbit is n_samples snapshots of n particles per coordinate, laid out
+ * [sample][particle] on the device (storage_4d_gpu's layout).  Windows are
+ * inclusive sample ranges [from[j], to[j]]; the full orbit is appended as a
+ * last window.  Output host double[n][2 (n_windows + 1)] = (tune_x,
+ * tune_y) per window.
+ *   method 0 -- Birkhoff tune (birkhoff_tune_vec, src/dynamic_indicator.cpp:
+ *     198-253): 1 - sum w_i dtheta_i / 2pi, theta = atan2(p, q), dtheta
+ *     wrapped by +2pi when negative, w = birkhoff_weights(to - from); NaN
+ *     when a window holds a NaN; full orbit = samples [0, n_samples-1].
+ *   method 1 -- FFT tune (fft_tune_vec, src/dynamic_indicator.cpp:255-330):
+ *     Hann-windowed FFT of q + i p (cuFFT), interpolated peak, |1 - nu|;
+ *     full orbit = samples [1, n_samples-1]. */
+hm_status hm_orbit_tunes(const double *x, const double *px, const double *y,
+                         const double *py, size_t n, size_t n_samples,
+                         const uint32_t *from, const uint32_t *to,
+                         size_t n_windows, int method, double *host_out);
+/* The same on host arrays [n_samples][n] (storage_4d::tune_birkhoff /
+ * tune_fft of the reference's host-side storage, src/henon.cu:3261-3329). */
+hm_status hm_orbit_tunes_host(const double *x, const double *px, const double *y,
+                              const double *py, size_t n, size_t n_samples,
+                              const uint32_t *from, const uint32_t *to,
+                              size_t n_windows, int method, double *host_out);
+/* Tracks n_turns turns recording the orbit (sample 0 = the current state),
+ * then Birkhoff tunes (and FFT tunes when fft_out is not NULL) of the
+ * windows plus the full orbit, with each orbit's mean removed first when
+ * remove_mean: henon_tracker::birkhoff_tunes (remove_mean 0) and
+ * ::all_tunes (remove_mean 1), src/henon.cu:2890-3078.  Outputs host
+ * double[n_total][2 (n_windows + 1)]. */
+hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turns,
+                                 double mu, double barrier, const uint32_t *from,
+                                 const uint32_t *to, size_t n_windows,
+                                 int remove_mean, double *birkhoff_out,
+                                 double *fft_out);
+/* Tunes of a storage's snapshots (storage_4d::tune_birkhoff / tune_fft,
+ * src/henon.cu:3261-3329). */
+hm_status hm_storage_tunes(const hm_storage *s, const uint32_t *from,
+                           const uint32_t *to, size_t n_windows, int method,
+                           double *host_out);
 
 /* ---- orbit-loss gradients (reverse-mode adjoint) ---------------------------
  * No counterpart in the reference (its tangent map is forward only,

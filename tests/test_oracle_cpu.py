@@ -98,6 +98,39 @@ def test_indicator_oracle_pinned():
     assert np.isnan(L.m_l3).any() and np.isfinite(L.m_l3).any()
 
 
+def test_tune_oracle_reproduces_notebook_values():
+    from oracle import tunes as T
+
+    nb = golden_json("notebook_values.json")["tunes_0p1_eps0"]
+    tabs = O.tables(10000, *TUNES, "sps", epsilon=0.0)
+    orb = T.remove_mean(T.orbit([0.1], [0.0], [0.1], [0.0], tabs, 10000, 0.0, 10.0))
+    x, px, y, py = (orb[c, :, 0] for c in range(4))
+
+    def window(key):
+        a, b = (int(v) for v in key.split("-"))
+        return slice(a, b + 1)
+
+    for key, v in nb["birkhoff_x"].items():
+        s = window(key)
+        assert T.birkhoff_tune(x[s], px[s]) == v, key
+    for key, v in nb["fft_x"].items():
+        s = window(key)
+        assert T.fft_tune(x[s], px[s]) == v, key
+    for key, v in nb["fft_y"].items():
+        s = window(key)
+        assert T.fft_tune(y[s], py[s]) == v, key
+    for key, v in nb["birkhoff_y_approx"].items():
+        s = window(key)
+        assert abs(T.birkhoff_tune(y[s], py[s]) - v) < 1e-10, key
+    # windows + full orbit layout, NaN handling
+    b = T.tune_vec(x, px, y, py, [0, 500], [500, 1000], "birkhoff")
+    assert len(b) == 6 and b[0] == nb["birkhoff_x"]["0-500"]
+    xn = x.copy()
+    xn[700] = np.nan
+    b = T.tune_vec(xn, px, y, py, [0, 500], [500, 1000], "fft")
+    assert np.isnan(b[2]) and np.isnan(b[3]) and not np.isnan(b[0]) and np.isnan(b[4])
+
+
 @pytest.mark.skipif(O.reference_module("fmad_off") is None, reason="reference build absent")
 @pytest.mark.parametrize("eps,mu,nt", [(0.0, 0.0, 1500), (16.0, 0.2, 1500), (64.0, -0.3, 1200)])
 def test_oracle_equals_reference_build_live(eps, mu, nt):
