@@ -64,6 +64,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched / adjoint / indicator measurements")
+    ap.add_argument("--stage-turns", type=int, default=None,
+                    help="turn records per staged bulk copy (0: direct reads; "
+                         "default: the library's setting)")
     return ap.parse_args()
 
 
@@ -73,6 +76,7 @@ def workload_config(args, n_gpus):
             "particles_per_gpu": args.side * args.side, "turns": args.turns,
             "epsilon": list(EPSILONS), "mu": list(MUS), "tunes": list(TUNES),
             "arith": args.arith, "parallelism": f"particle shards x{n_gpus}",
+            "table_staging": args.stage_turns,
             "l2": "flushed between steps (256 MiB write); state < L2, compute-bound"}
 
 
@@ -391,6 +395,9 @@ def run_ours(args):
     from henon_map_cpp_b200 import _capi as C  # fails loudly if the library is missing
 
     arith = C.ARITH_FAST if args.arith == "fast" else C.ARITH_EXACT
+    if args.stage_turns is not None:
+        C.set_track_staging(args.stage_turns)
+    args.stage_turns = C.get_track_staging()
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
 
@@ -479,6 +486,19 @@ def run_ours(args):
         o_ms = float(t.item())
     o_value = float(n) * args.turns * 6 * world / (o_ms * 1e-3)
 
+    # Turn records read directly vs staged through shared memory by bulk
+    # copies (one step each, same workload and arithmetic).
+    staging = None
+    if world == 1 and not args.no_extras:
+        staging = {"workload": "the headline step, one timed step per setting",
+                   "unit": "achieved FP64 TFLOP/s of track_chunk_kernel"}
+        default_stage = C.get_track_staging()
+        for st in (0, 64, 256, 512):
+            C.set_track_staging(st)
+            _, _, s_flops, s_kms, _ = timed(arith, 1, 1)
+            staging[str(st)] = s_flops / (s_kms * 1e-3) / 1e12 if s_kms > 0 else None
+        C.set_track_staging(default_stage)
+
     # End to end through the public API with host buffers.
     e2e = None
     if not args.no_e2e:
@@ -540,6 +560,7 @@ def run_ours(args):
             "other_arith": {"arith": "fast" if other == C.ARITH_FAST else "exact",
                             "value": o_value, "achieved_tflops": o_tf,
                             "frac": o_tf / peak_tflops if peak_tflops else None},
+            "table_staging": staging,
             "gpu_launches": launches,
             "clocks": clock_summary,
             "e2e": e2e,

@@ -61,6 +61,8 @@ _SIGNATURES = {
     "hm_set_cancel_callback": (None, [c_void_p, c_void_p]),
     "hm_set_track_config": (None, [c_int, c_int, c_uint32, c_uint32]),
     "hm_get_track_config": (None, [POINTER(c_int), POINTER(c_int), _PU32, _PU32]),
+    "hm_set_track_staging": (None, [c_uint32]),
+    "hm_get_track_staging": (None, [_PU32]),
     "hm_modulation": (None, [c_char_p, c_uint32, c_double, c_double, c_double, c_double,
                              c_uint32, _PD, _PD]),
     "hm_sps_modulation": (None, [c_double, c_double, ctypes.c_int32, ctypes.c_int32, _PD]),
@@ -669,6 +671,18 @@ def get_track_config():
     call("hm_get_track_config", ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
          ctypes.byref(d))
     return int(a.value), int(b.value), int(c.value), int(d.value)
+
+
+def set_track_staging(stage_turns: int) -> None:
+    """0: turn records read from global memory; else staged into shared
+    memory by bulk copies, stage_turns turns at a time."""
+    call("hm_set_track_staging", int(stage_turns))
+
+
+def get_track_staging() -> int:
+    v = c_uint32()
+    call("hm_get_track_staging", ctypes.byref(v))
+    return int(v.value)
 
 
 def set_profiling(on: bool) -> None:

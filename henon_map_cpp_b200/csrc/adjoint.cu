@@ -29,9 +29,10 @@ namespace {
 
 using dev::Rn;
 
+// r < barrier^2 on the radius the loss uses (see dev::Barrier for the
+// bit-pattern compare).
 __device__ __forceinline__ bool inside(double r, long long b2bits) {
-    return static_cast<unsigned long long>(__double_as_longlong(r)) <
-           static_cast<unsigned long long>(b2bits);
+    return dev::pattern(r) < static_cast<unsigned long long>(b2bits);
 }
 
 struct S4 {
@@ -42,36 +43,10 @@ struct S4 {
 // tracker's grouping (the loss uses the same number).
 template <int ARITH, bool OCT>
 __device__ __forceinline__ double fwd(S4 &s, const dev::Turn &t, double mu) {
-    const double x = s.x, y = s.y;
-    double px, py, X, PX, Y, PY;
-    if (ARITH == HM_ARITH_EXACT) {
-        const double xx = Rn::mul(x, x), yy = Rn::mul(y, y);
-        px = Rn::add(s.px, Rn::sub(xx, yy));
-        py = Rn::add(s.py, Rn::mul(Rn::mul(-2.0, x), y));
-        if (OCT) {
-            px = Rn::add(px, Rn::mul(mu, Rn::sub(Rn::mul(xx, x), Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
-            py = Rn::add(py, Rn::mul(mu, Rn::sub(Rn::mul(yy, y), Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
-        }
-        X = Rn::add(Rn::mul(x, t.cx), Rn::mul(px, t.sx));
-        PX = Rn::add(Rn::mul(-x, t.sx), Rn::mul(px, t.cx));
-        Y = Rn::add(Rn::mul(y, t.cy), Rn::mul(py, t.sy));
-        PY = Rn::add(Rn::mul(-y, t.sy), Rn::mul(py, t.cy));
-        s = S4{X, PX, Y, PY};
-        return Rn::add(Rn::add(Rn::mul(X, X), Rn::mul(PX, PX)), Rn::add(Rn::mul(Y, Y), Rn::mul(PY, PY)));
-    }
-    const double xx = x * x, yy = y * y;
-    px = s.px + (xx - yy);
-    py = fma(-2.0 * x, y, s.py);
-    if (OCT) {
-        px = fma(mu * x, fma(-3.0, yy, xx), px);
-        py = fma(mu * y, fma(-3.0, xx, yy), py);
-    }
-    X = fma(x, t.cx, px * t.sx);
-    PX = fma(px, t.cx, -x * t.sx);
-    Y = fma(y, t.cy, py * t.sy);
-    PY = fma(py, t.cy, -y * t.sy);
-    s = S4{X, PX, Y, PY};
-    return fma(PX, PX, X * X) + fma(PY, PY, Y * Y);
+    dev::Particle p = dev::make_particle(s.x, s.px, s.y, s.py);
+    const double r = dev::turn<ARITH, OCT, false>(p, t, mu);
+    s = S4{p.x, p.px, p.y, p.py};
+    return ARITH == HM_ARITH_EXACT ? dev::radius_exact(p) : r;
 }
 
 __device__ __forceinline__ void store4(double *buf, size_t slot, size_t n, size_t i, const S4 &s) {

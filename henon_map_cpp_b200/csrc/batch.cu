@@ -25,65 +25,7 @@
 namespace hm {
 namespace {
 
-using dev::Rn;
-
-__device__ __forceinline__ bool inside(double r, long long b2bits) {
-    return static_cast<unsigned long long>(__double_as_longlong(r)) <
-           static_cast<unsigned long long>(b2bits);
-}
-
-struct P {
-    double x, px, y, py, xx, yy;
-};
-
-template <bool OCT>
-__device__ __forceinline__ double turn_exact(P &p, const dev::Turn &t, double mu) {
-    double px = Rn::add(p.px, Rn::sub(p.xx, p.yy));
-    double py = Rn::add(p.py, Rn::mul(Rn::mul(-2.0, p.x), p.y));
-    if (OCT) {
-        px = Rn::add(px, Rn::mul(mu, Rn::sub(Rn::mul(p.xx, p.x),
-                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.y), p.y), p.x))));
-        py = Rn::add(py, Rn::mul(mu, Rn::sub(Rn::mul(p.yy, p.y),
-                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.x), p.x), p.y))));
-    }
-    const double x = Rn::add(Rn::mul(p.x, t.cx), Rn::mul(px, t.sx));
-    px = Rn::add(Rn::mul(-p.x, t.sx), Rn::mul(px, t.cx));
-    const double y = Rn::add(Rn::mul(p.y, t.cy), Rn::mul(py, t.sy));
-    py = Rn::add(Rn::mul(-p.y, t.sy), Rn::mul(py, t.cy));
-    p.xx = Rn::mul(x, x);
-    p.yy = Rn::mul(y, y);
-    p.x = x;
-    p.px = px;
-    p.y = y;
-    p.py = py;
-    return Rn::add(Rn::add(p.xx, Rn::mul(px, px)), Rn::add(p.yy, Rn::mul(py, py)));
-}
-
-template <bool OCT>
-__device__ __forceinline__ double turn_fast(P &p, const dev::Turn &t, double mu) {
-    double px = p.px + (p.xx - p.yy);
-    double py = fma(-2.0 * p.x, p.y, p.py);
-    if (OCT) {
-        px = fma(mu * p.x, fma(-3.0, p.yy, p.xx), px);
-        py = fma(mu * p.y, fma(-3.0, p.xx, p.yy), py);
-    }
-    const double x = fma(p.x, t.cx, px * t.sx);
-    px = fma(px, t.cx, -p.x * t.sx);
-    const double y = fma(p.y, t.cy, py * t.sy);
-    py = fma(py, t.cy, -p.y * t.sy);
-    p.xx = x * x;
-    p.yy = y * y;
-    p.x = x;
-    p.px = px;
-    p.y = y;
-    p.py = py;
-    return fma(px, px, p.xx) + fma(py, py, p.yy);
-}
-
-template <int ARITH, bool OCT>
-__device__ __forceinline__ double one_turn(P &p, const dev::Turn &t, double mu) {
-    return ARITH == HM_ARITH_EXACT ? turn_exact<OCT>(p, t, mu) : turn_fast<OCT>(p, t, mu);
-}
+using dev::Particle;
 
 // Copies every non-NaN particle of every set into list 0 of its set and
 // counts them (check_nan: NaN particles are never touched).
@@ -142,7 +84,7 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
                                          const BatchStateDev &st, uint32_t s, uint32_t start,
                                          int in, int out) {
     const unsigned lane = threadIdx.x & 31u;
-    P p[K];
+    Particle p[K];
     uint64_t id[K];
     bool live[K];
     bool any = false;
@@ -152,28 +94,32 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
         live[j] = e < st.live;
         const uint64_t slot = set.list_offset + (live[j] ? e : 0u);
         id[j] = b.list_idx[in][slot];
-        const double x = b.list_x[in][slot], y = b.list_y[in][slot];
-        p[j] = P{x, b.list_px[in][slot], y, b.list_py[in][slot], Rn::mul(x, x), Rn::mul(y, y)};
+        p[j] = dev::make_particle(b.list_x[in][slot], b.list_px[in][slot], b.list_y[in][slot],
+                                  b.list_py[in][slot]);
         any |= live[j];
     }
     const uint32_t turn0 = st.done, nt = st.turns;
     const double mu = set.mu;
+    const dev::Barrier bar = dev::make_barrier<ARITH>(set.b2bits);
     bool warp_live = __any_sync(dev::kFullMask, any);
+    dev::Turn t = nt ? dev::load_turn(set.table, turn0) : dev::Turn{0.0, 0.0, 0.0, 0.0};
     for (uint32_t k = 0; warp_live && k < nt; ++k) {
-        const dev::Turn t = dev::load_turn(set.table, turn0 + k);
-        bool any_lost = false;
-        bool lost[K];
+        const uint32_t kn = (k + 1 < nt) ? k + 1 : k;
+        const dev::Turn tn = dev::load_turn(set.table, turn0 + kn);
+        bool any_check = false;
+        bool check[K];
+        double r[K];
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            const double r = one_turn<ARITH, OCT>(p[j], t, mu);
-            lost[j] = live[j] && !inside(r, set.b2bits);
-            any_lost |= lost[j];
+            r[j] = dev::turn<ARITH, OCT, false>(p[j], t, mu);
+            check[j] = live[j] && !dev::surely_inside(r[j], bar);
+            any_check |= check[j];
         }
-        if (__any_sync(dev::kFullMask, any_lost)) {
+        if (__any_sync(dev::kFullMask, any_check)) {
             bool still = false;
 #pragma unroll
             for (int j = 0; j < K; ++j) {
-                if (lost[j]) {
+                if (check[j] && !dev::settle_inside<ARITH>(r[j], p[j], bar)) {
                     b.x[id[j]] = b.px[id[j]] = b.y[id[j]] = b.py[id[j]] = dev::quiet_nan();
                     b.steps[id[j]] = turn0 + k;
                     live[j] = false;
@@ -182,6 +128,7 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
             }
             warp_live = __any_sync(dev::kFullMask, still);
         }
+        t = tn;
     }
     const bool final_chunk = turn0 + nt == set.n_turns;
 #pragma unroll

@@ -29,35 +29,6 @@ namespace {
 
 using dev::Rn;
 
-__device__ __forceinline__ bool inside(double r, long long b2bits) {
-    return static_cast<unsigned long long>(__double_as_longlong(r)) <
-           static_cast<unsigned long long>(b2bits);
-}
-
-// One forward turn in the reference order (henon_step, src/henon.cu:482-542).
-template <bool OCT>
-__device__ __forceinline__ double map_turn(double &x, double &px, double &y, double &py,
-                                           const dev::Turn &t, double mu) {
-    const double xx = Rn::mul(x, x), yy = Rn::mul(y, y);
-    double npx = Rn::add(px, Rn::sub(xx, yy));
-    double npy = Rn::add(py, Rn::mul(Rn::mul(-2.0, x), y));
-    if (OCT) {
-        npx = Rn::add(npx, Rn::mul(mu, Rn::sub(Rn::mul(xx, x),
-                                               Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
-        npy = Rn::add(npy, Rn::mul(mu, Rn::sub(Rn::mul(yy, y),
-                                               Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
-    }
-    const double nx = Rn::add(Rn::mul(x, t.cx), Rn::mul(npx, t.sx));
-    npx = Rn::add(Rn::mul(-x, t.sx), Rn::mul(npx, t.cx));
-    const double ny = Rn::add(Rn::mul(y, t.cy), Rn::mul(npy, t.sy));
-    npy = Rn::add(Rn::mul(-y, t.sy), Rn::mul(npy, t.cy));
-    x = nx;
-    px = npx;
-    y = ny;
-    py = npy;
-    return Rn::add(Rn::add(Rn::mul(x, x), Rn::mul(px, px)), Rn::add(Rn::mul(y, y), Rn::mul(py, py)));
-}
-
 template <bool OCT, bool DO_M, bool DO_V, bool DO_T>
 __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     extern __shared__ double smem[];
@@ -117,6 +88,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     }
 
     const double mu = a.mu;
+    const dev::Barrier bar = dev::make_barrier<HM_ARITH_EXACT>(a.b2bits);
     bool warp_live = __any_sync(dev::kFullMask, alive);
     uint32_t k = 0;
     for (; k < a.n_turns && warp_live; ++k) {
@@ -129,9 +101,14 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
         // ---- track(p, 1) ------------------------------------------------------
         if (alive) {
             const dev::Turn t = dev::load_turn(a.table, a.live_step + k);
-            const double r = map_turn<OCT>(x, px, y, py, t, mu);
-            if (inside(r, a.b2bits)) {
+            dev::Particle q = dev::make_particle(x, px, y, py);
+            const double r = dev::turn<HM_ARITH_EXACT, OCT, false>(q, t, mu);
+            if (dev::inside<HM_ARITH_EXACT>(r, q, bar)) {
                 steps += 1u;
+                x = q.x;
+                px = q.px;
+                y = q.y;
+                py = q.py;
             } else {
                 x = px = y = py = dev::quiet_nan();
                 alive = false;

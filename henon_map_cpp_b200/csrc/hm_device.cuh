@@ -5,6 +5,8 @@
 
 #include <cstdint>
 
+#include "../../include/henon_b200.h"
+
 namespace hm {
 namespace dev {
 
@@ -38,6 +40,241 @@ __device__ __forceinline__ Turn load_turn(const double *table, uint32_t i) {
 
 __device__ __forceinline__ bool is_lost(double x, double px, double y, double py) {
     return isnan(x) || isnan(px) || isnan(y) || isnan(py);
+}
+
+// ---- bulk copies into shared memory ---------------------------------------------
+// cp.async.bulk (the untiled TMA copy, no multicast) from this GPU's global
+// memory into the CTA's shared memory, completed on an mbarrier by
+// transaction count.  Source, destination and size must be multiples of 16
+// bytes.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+// Makes mbarrier initialisation visible to the async proxy (TMA).
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this CTA's earlier shared-memory accesses before later async-proxy
+// writes (a bulk copy refilling a buffer that threads have read).
+__device__ __forceinline__ void async_proxy_fence() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0u;
+}
+
+// Waits for the phase with the given parity to complete; gives up (returns
+// false) after kWaitPolls polls or about two seconds, whichever comes first,
+// so that a copy that never lands cannot hang the GPU.
+constexpr uint32_t kWaitPolls = 1u << 24;
+constexpr long long kWaitCycles = 4000000000ll;
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    const long long t0 = clock64();
+    for (uint32_t i = 0; i < kWaitPolls; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (clock64() - t0 > kWaitCycles) break;
+    }
+    return false;
+}
+
+// ---- the map ------------------------------------------------------------------
+// Particle in registers; xx = x*x and yy = y*y of the current coordinates
+// are carried from one turn's barrier test into the next turn's kicks (the
+// reference computes the same products twice).
+struct Particle {
+    double x, px, y, py, xx, yy;
+};
+
+__device__ __forceinline__ Particle make_particle(double x, double px, double y, double py) {
+    return Particle{x, px, y, py, Rn::mul(x, x), Rn::mul(y, y)};
+}
+
+// x^2+px^2+y^2+py^2 grouped as (x*x + px*px) + (y*y + py*py), separately
+// rounded: the radius of check_barrier, src/henon.cu:113-116.
+__device__ __forceinline__ double radius_exact(const Particle &p) {
+    return Rn::add(Rn::add(p.xx, Rn::mul(p.px, p.px)), Rn::add(p.yy, Rn::mul(p.py, p.py)));
+}
+
+// The same sum with two fused multiply-adds: three FP64 instructions
+// instead of five, within 2 ulp of the exact sum (all terms are >= 0).
+__device__ __forceinline__ double radius_fma(const Particle &p) {
+    return fma(p.px, p.px, p.xx) + fma(p.py, p.py, p.yy);
+}
+
+// Forward turn in the reference order: sextupole, [octupole], rotate x then
+// y with table[steps] (henon_step, src/henon.cu:493-508, primitives
+// :131-173).  Returns radius_fma of the new state.
+template <bool OCT>
+__device__ __forceinline__ double turn_exact_fwd(Particle &p, const Turn &t, double mu) {
+    // px += x*x - y*y ; py += (-2*x)*y          (sextupole, :131-143)
+    double px = Rn::add(p.px, Rn::sub(p.xx, p.yy));
+    double py = Rn::add(p.py, Rn::mul(Rn::mul(-2.0, p.x), p.y));
+    if (OCT) {
+        // px += mu*((x*x*x) - ((3*y)*y)*x), py likewise   (octupole, :145-157)
+        px = Rn::add(px, Rn::mul(mu, Rn::sub(Rn::mul(p.xx, p.x),
+                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.y), p.y), p.x))));
+        py = Rn::add(py, Rn::mul(mu, Rn::sub(Rn::mul(p.yy, p.y),
+                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.x), p.x), p.y))));
+    }
+    // x' = x*c + px*s ; px' = (-x)*s + px*c       (rotation, :159-173)
+    const double x = Rn::add(Rn::mul(p.x, t.cx), Rn::mul(px, t.sx));
+    px = Rn::add(Rn::mul(-p.x, t.sx), Rn::mul(px, t.cx));
+    const double y = Rn::add(Rn::mul(p.y, t.cy), Rn::mul(py, t.sy));
+    py = Rn::add(Rn::mul(-p.y, t.sy), Rn::mul(py, t.cy));
+    p = Particle{x, px, y, py, Rn::mul(x, x), Rn::mul(y, y)};
+    return radius_fma(p);
+}
+
+// Reverse turn: rotate x then y backwards with table[steps-1], subtract the
+// octupole, subtract the sextupole (src/henon.cu:510-528).
+template <bool OCT>
+__device__ __forceinline__ double turn_exact_rev(Particle &p, const Turn &t, double mu) {
+    const double x = Rn::sub(Rn::mul(p.x, t.cx), Rn::mul(p.px, t.sx));
+    double px = Rn::add(Rn::mul(p.x, t.sx), Rn::mul(p.px, t.cx));
+    const double y = Rn::sub(Rn::mul(p.y, t.cy), Rn::mul(p.py, t.sy));
+    double py = Rn::add(Rn::mul(p.y, t.sy), Rn::mul(p.py, t.cy));
+    const double xx = Rn::mul(x, x);
+    const double yy = Rn::mul(y, y);
+    if (OCT) {
+        px = Rn::sub(px, Rn::mul(mu, Rn::sub(Rn::mul(xx, x),
+                                             Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
+        py = Rn::sub(py, Rn::mul(mu, Rn::sub(Rn::mul(yy, y),
+                                             Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
+    }
+    px = Rn::sub(px, Rn::sub(xx, yy));
+    py = Rn::sub(py, Rn::mul(Rn::mul(-2.0, x), y));
+    p = Particle{x, px, y, py, xx, yy};
+    return radius_fma(p);
+}
+
+// The same map with fused multiply-adds and x^3-3xy^2 = x(x^2-3y^2): 14 + 3
+// (mu = 0) / 20 + 3 (mu != 0) FP64 instructions per particle-turn, against
+// 19 + 3 / 33 + 3 for the exact turn.
+template <bool OCT>
+__device__ __forceinline__ double turn_fast_fwd(Particle &p, const Turn &t, double mu) {
+    double px = p.px + (p.xx - p.yy);
+    double py = fma(-2.0 * p.x, p.y, p.py);
+    if (OCT) {
+        px = fma(mu * p.x, fma(-3.0, p.yy, p.xx), px);
+        py = fma(mu * p.y, fma(-3.0, p.xx, p.yy), py);
+    }
+    const double x = fma(p.x, t.cx, px * t.sx);
+    px = fma(px, t.cx, -p.x * t.sx);
+    const double y = fma(p.y, t.cy, py * t.sy);
+    py = fma(py, t.cy, -p.y * t.sy);
+    p = Particle{x, px, y, py, x * x, y * y};
+    return radius_fma(p);
+}
+
+template <bool OCT>
+__device__ __forceinline__ double turn_fast_rev(Particle &p, const Turn &t, double mu) {
+    const double x = fma(p.x, t.cx, -p.px * t.sx);
+    double px = fma(p.x, t.sx, p.px * t.cx);
+    const double y = fma(p.y, t.cy, -p.py * t.sy);
+    double py = fma(p.y, t.sy, p.py * t.cy);
+    const double xx = x * x;
+    const double yy = y * y;
+    if (OCT) {
+        px = fma(-mu * x, fma(-3.0, yy, xx), px);
+        py = fma(-mu * y, fma(-3.0, xx, yy), py);
+    }
+    px = px - (xx - yy);
+    py = fma(2.0 * x, y, py);
+    p = Particle{x, px, y, py, xx, yy};
+    return radius_fma(p);
+}
+
+// One turn; returns radius_fma of the new state for the barrier test below.
+template <int ARITH, bool OCT, bool REV>
+__device__ __forceinline__ double turn(Particle &p, const Turn &t, double mu) {
+    if (ARITH == HM_ARITH_EXACT)
+        return REV ? turn_exact_rev<OCT>(p, t, mu) : turn_exact_fwd<OCT>(p, t, mu);
+    return REV ? turn_fast_rev<OCT>(p, t, mu) : turn_fast_fwd<OCT>(p, t, mu);
+}
+
+// ---- the barrier test ------------------------------------------------------------
+// A particle is kept while r < barrier^2 (check_barrier, src/henon.cu:
+// 113-116).  r is a sum of squares, so it is +0, positive, +inf or NaN, and
+// the comparison is an unsigned compare of bit patterns: non-negative
+// doubles order like their patterns and every NaN pattern, of either sign,
+// lies above +inf's, so NaN particles are lost exactly when
+// `r < barrier_pow_2` is false.  The test stays off the FP64 pipe.
+//
+// In exact arithmetic the decision must be the one the separately rounded
+// sum radius_exact gives.  It is taken from radius_fma instead whenever
+// radius_fma lies more than kBarrierMargin patterns below barrier^2: the
+// two sums are within 2 + 3 rounding errors of the same non-negative real
+// sum, i.e. within ~6 representable doubles of each other (subnormal and
+// overflowing sums included), so a margin of 64 decides the same way.
+// Inside the margin (or above it, where the particle may be lost) the
+// caller settles the test with radius_exact.  Fast arithmetic uses
+// radius_fma itself (margin 0).
+constexpr unsigned long long kBarrierMargin = 64ull;
+
+struct Barrier {
+    unsigned long long b2;  // pattern of barrier^2 (0 for a NaN barrier)
+    unsigned long long lo;  // patterns below lo: inside for certain
+    unsigned long long hi;  // exact arithmetic: patterns above hi are outside
+};
+
+template <int ARITH>
+__device__ __forceinline__ Barrier make_barrier(long long b2bits) {
+    const unsigned long long b2 = static_cast<unsigned long long>(b2bits);
+    if (ARITH != HM_ARITH_EXACT) return Barrier{b2, b2, b2};
+    const unsigned long long lo = b2 > kBarrierMargin ? b2 - kBarrierMargin : 0ull;
+    const unsigned long long hi = b2 < ~0ull - kBarrierMargin ? b2 + kBarrierMargin : ~0ull;
+    return Barrier{b2, lo, hi};
+}
+
+__device__ __forceinline__ unsigned long long pattern(double r) {
+    return static_cast<unsigned long long>(__double_as_longlong(r));
+}
+
+// Common case: r_fma decides "inside" on its own.
+__device__ __forceinline__ bool surely_inside(double r_fma, const Barrier &b) {
+    return pattern(r_fma) < b.lo;
+}
+
+// The rest: the reference's decision for a particle whose r_fma did not
+// pass surely_inside.
+template <int ARITH>
+__device__ __forceinline__ bool settle_inside(double r_fma, const Particle &p, const Barrier &b) {
+    if (ARITH != HM_ARITH_EXACT) return false;
+    return pattern(r_fma) <= b.hi && pattern(radius_exact(p)) < b.b2;
+}
+
+template <int ARITH>
+__device__ __forceinline__ bool inside(double r_fma, const Particle &p, const Barrier &b) {
+    return surely_inside(r_fma, b) || settle_inside<ARITH>(r_fma, p, b);
 }
 
 // Jacobian of one turn, row-major, in the reference's expression order

@@ -132,6 +132,11 @@ struct TrackChunk {
     uint32_t steps_final;  // steps written for survivors of the last chunk
     double mu;
     long long b2bits;      // bit pattern of barrier^2 (0 when NaN)
+    // 0: turn records read from global memory; otherwise records are
+    // staged through shared memory by bulk copies, this many turns a stage
+    // (a power of two in [16, 512]; needs a 16-byte aligned table).
+    uint32_t stage_turns;
+    uint32_t *fault;       // set to nonzero when a staged copy timed out
 };
 
 struct TrackLaunch {

@@ -17,178 +17,153 @@
 
 #include <cstdint>
 
+#include "hm_device.cuh"
 #include "hm_internal.h"
 
 namespace hm {
 namespace {
 
-constexpr unsigned kFullMask = 0xffffffffu;
+using dev::Barrier;
+using dev::kFullMask;
+using dev::Particle;
+using dev::quiet_nan;
+using dev::Rn;
+using dev::Turn;
 
-__device__ __forceinline__ double quiet_nan() {
-    return __longlong_as_double(0x7ff8000000000000LL);  // glibc NAN
+// One turn of the K particles of a thread.  The common case costs the map
+// and one integer compare per particle; a warp with a particle near or past
+// the barrier takes the rare path, which settles the test and freezes lost
+// particles (set_to_nan, src/henon.cu:123-129) with steps = the turns they
+// survived.
+template <int ARITH, bool OCT, bool REV, int K>
+__device__ __forceinline__ void turn_all(const TrackChunk &c, const Barrier &bar, double mu,
+                                         const Turn &t, uint32_t k, Particle (&p)[K],
+                                         const uint32_t (&id)[K], bool (&live)[K],
+                                         bool &warp_live) {
+    double r[K];
+    bool check[K];
+    bool any_check = false;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        r[j] = dev::turn<ARITH, OCT, REV>(p[j], t, mu);
+        check[j] = live[j] && !dev::surely_inside(r[j], bar);
+        any_check |= check[j];
+    }
+    if (__any_sync(kFullMask, any_check)) {
+        const uint32_t s = REV ? c.turn0 - k : c.turn0 + k;
+        bool any_live = false;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (check[j] && !dev::settle_inside<ARITH>(r[j], p[j], bar)) {
+                const uint32_t i = id[j];
+                c.ux[i] = quiet_nan();
+                c.upx[i] = quiet_nan();
+                c.uy[i] = quiet_nan();
+                c.upy[i] = quiet_nan();
+                c.usteps[i] = s;
+                live[j] = false;
+            }
+            any_live |= live[j];
+        }
+        warp_live = __any_sync(kFullMask, any_live);
+    }
 }
 
-// Separately rounded binary64 operations; the __d*_rn intrinsics are never
-// contracted into fused multiply-adds, so a sequence of them reproduces the
-// host's SSE2 arithmetic bit for bit.
-struct Rn {
-    static __device__ __forceinline__ double mul(double a, double b) {
-        return __dmul_rn(a, b);
+// The chunk's turns with the turn records read from global memory: every
+// lane of a warp loads the same 32-byte record (one broadcast transaction,
+// an L1 hit after the first warp), prefetched one turn ahead.
+template <int ARITH, bool OCT, bool REV, int K>
+__device__ __forceinline__ void turns_direct(const TrackChunk &c, const Barrier &bar,
+                                             Particle (&p)[K], const uint32_t (&id)[K],
+                                             bool (&live)[K], bool warp_live) {
+    const double mu = c.mu;
+    const uint32_t nt = c.n_turns;
+    Turn t = nt ? dev::load_turn(c.table, REV ? c.turn0 - 1u : c.turn0) : Turn{0.0, 0.0, 0.0, 0.0};
+    for (uint32_t k = 0; warp_live && k < nt; ++k) {
+        const uint32_t kn = (k + 1 < nt) ? k + 1 : k;
+        const Turn tn = dev::load_turn(c.table, REV ? c.turn0 - 1u - kn : c.turn0 + kn);
+        turn_all<ARITH, OCT, REV, K>(c, bar, mu, t, k, p, id, live, warp_live);
+        t = tn;
     }
-    static __device__ __forceinline__ double add(double a, double b) {
-        return __dadd_rn(a, b);
-    }
-    static __device__ __forceinline__ double sub(double a, double b) {
-        return __dsub_rn(a, b);
-    }
-};
-
-struct Turn {
-    double sx, cx, sy, cy;
-};
-
-__device__ __forceinline__ Turn load_turn(const double *table, uint32_t i) {
-    const double2 *p = reinterpret_cast<const double2 *>(table) + 2 * size_t(i);
-    const double2 a = __ldg(p);
-    const double2 b = __ldg(p + 1);
-    return Turn{a.x, a.y, b.x, b.y};
 }
 
-// Particle in registers; xx = x*x and yy = y*y of the current coordinates
-// are carried from the barrier test of one turn into the kicks of the next
-// (the reference computes the same products twice).
-struct Particle {
-    double x, px, y, py, xx, yy;
-};
-
-// ---- one turn, reference order ---------------------------------------------
-// Forward: sextupole, [octupole], rotate x then y with table[steps]
-// (src/henon.cu:493-508).  Returns x^2+px^2+y^2+py^2 grouped as
-// (x*x + px*px) + (y*y + py*py) (check_barrier, src/henon.cu:113-116).
-template <bool OCT>
-__device__ __forceinline__ double turn_exact_fwd(Particle &p, const Turn &t,
-                                                 double mu) {
-    // px += x*x - y*y ; py += (-2*x)*y          (sextupole, :131-143)
-    double px = Rn::add(p.px, Rn::sub(p.xx, p.yy));
-    double py = Rn::add(p.py, Rn::mul(Rn::mul(-2.0, p.x), p.y));
-    if (OCT) {
-        // px += mu*((x*x*x) - ((3*y)*y)*x), py likewise   (octupole, :145-157)
-        px = Rn::add(px, Rn::mul(mu, Rn::sub(Rn::mul(p.xx, p.x),
-                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.y), p.y), p.x))));
-        py = Rn::add(py, Rn::mul(mu, Rn::sub(Rn::mul(p.yy, p.y),
-                                             Rn::mul(Rn::mul(Rn::mul(3.0, p.x), p.x), p.y))));
+// The chunk's turns with the turn records staged in shared memory: the
+// chunk is cut into stages of c.stage_turns turns whose records (a
+// contiguous span of the table) one thread brings in with a bulk copy,
+// double-buffered, so that the copy of stage s+1 overlaps the turns of
+// stage s.  Every warp then reads each record from shared memory as a
+// broadcast.  Warps whose particles are all lost keep taking part in the
+// per-stage barriers; the block stops when none of its warps is live.
+// Returns false when a copy did not land within the bounded wait (the
+// chunk's results are then invalid and c.fault is set).
+template <int ARITH, bool OCT, bool REV, int K>
+__device__ __forceinline__ bool turns_staged(const TrackChunk &c, const Barrier &bar,
+                                             Particle (&p)[K], const uint32_t (&id)[K],
+                                             bool (&live)[K], bool warp_live) {
+    extern __shared__ __align__(128) double stage_buf[];  // [2][S][4]
+    __shared__ __align__(8) uint64_t full[2];
+    const double mu = c.mu;
+    const uint32_t nt = c.n_turns, S = c.stage_turns;
+    const uint32_t n_stages = (nt + S - 1) / S;
+    const bool leader = threadIdx.x == 0;
+    auto issue = [&](uint32_t st) {
+        const uint32_t k0 = st * S;
+        const uint32_t kn = min(S, nt - k0);
+        const uint32_t lo = REV ? c.turn0 - k0 - kn : c.turn0 + k0;
+        dev::bulk_load(stage_buf + size_t(st & 1u) * S * 4u, c.table + size_t(lo) * 4u,
+                       kn * 32u, &full[st & 1u]);
+    };
+    if (leader) {
+        dev::mbar_init(&full[0], 1);
+        dev::mbar_init(&full[1], 1);
+        dev::mbar_init_fence();
     }
-    // x' = x*c + px*s ; px' = (-x)*s + px*c       (rotation, :159-173)
-    const double x = Rn::add(Rn::mul(p.x, t.cx), Rn::mul(px, t.sx));
-    px = Rn::add(Rn::mul(-p.x, t.sx), Rn::mul(px, t.cx));
-    const double y = Rn::add(Rn::mul(p.y, t.cy), Rn::mul(py, t.sy));
-    py = Rn::add(Rn::mul(-p.y, t.sy), Rn::mul(py, t.cy));
-    p.xx = Rn::mul(x, x);
-    p.yy = Rn::mul(y, y);
-    p.x = x;
-    p.px = px;
-    p.y = y;
-    p.py = py;
-    return Rn::add(Rn::add(p.xx, Rn::mul(px, px)), Rn::add(p.yy, Rn::mul(py, py)));
-}
-
-// Reverse: rotate x then y backwards with table[steps-1], subtract the
-// octupole, subtract the sextupole (src/henon.cu:510-528).
-template <bool OCT>
-__device__ __forceinline__ double turn_exact_rev(Particle &p, const Turn &t,
-                                                 double mu) {
-    const double x = Rn::sub(Rn::mul(p.x, t.cx), Rn::mul(p.px, t.sx));
-    double px = Rn::add(Rn::mul(p.x, t.sx), Rn::mul(p.px, t.cx));
-    const double y = Rn::sub(Rn::mul(p.y, t.cy), Rn::mul(p.py, t.sy));
-    double py = Rn::add(Rn::mul(p.y, t.sy), Rn::mul(p.py, t.cy));
-    const double xx = Rn::mul(x, x);
-    const double yy = Rn::mul(y, y);
-    if (OCT) {
-        px = Rn::sub(px, Rn::mul(mu, Rn::sub(Rn::mul(xx, x),
-                                             Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
-        py = Rn::sub(py, Rn::mul(mu, Rn::sub(Rn::mul(yy, y),
-                                             Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
+    __syncthreads();
+    if (leader) {
+        if (n_stages > 0) issue(0);
+        if (n_stages > 1) issue(1);
     }
-    px = Rn::sub(px, Rn::sub(xx, yy));
-    py = Rn::sub(py, Rn::mul(Rn::mul(-2.0, x), y));
-    p.x = x;
-    p.px = px;
-    p.y = y;
-    p.py = py;
-    p.xx = xx;
-    p.yy = yy;
-    return Rn::add(Rn::add(xx, Rn::mul(px, px)), Rn::add(yy, Rn::mul(py, py)));
-}
-
-// ---- one turn, fused multiply-adds ----------------------------------------
-// The same map with FMAs and x^3-3xy^2 = x(x^2-3y^2); 17 (mu=0) / 23 (mu!=0)
-// FP64 instructions per particle-turn instead of 24 / 38.
-template <bool OCT>
-__device__ __forceinline__ double turn_fast_fwd(Particle &p, const Turn &t,
-                                                double mu) {
-    double px = p.px + (p.xx - p.yy);
-    double py = fma(-2.0 * p.x, p.y, p.py);
-    if (OCT) {
-        px = fma(mu * p.x, fma(-3.0, p.yy, p.xx), px);
-        py = fma(mu * p.y, fma(-3.0, p.xx, p.yy), py);
+    bool timed_out = false;
+    uint32_t st = 0;
+    for (; st < n_stages; ++st) {
+        const uint32_t buf = st & 1u;
+        // Warp-uniform, so that the turn loop's warp votes see every lane.
+        const bool landed = dev::mbar_wait(&full[buf], (st >> 1) & 1u);
+        if (!__all_sync(kFullMask, landed)) timed_out = true;
+        const uint32_t k0 = st * S;
+        const uint32_t kn = min(S, nt - k0);
+        const double *rec = stage_buf + size_t(buf) * S * 4u;
+        if (!timed_out) {
+            for (uint32_t kk = 0; warp_live && kk < kn; ++kk) {
+                const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * (REV ? kn - 1u - kk : kk));
+                const double2 a = q[0], b = q[1];
+                turn_all<ARITH, OCT, REV, K>(c, bar, mu, Turn{a.x, a.y, b.x, b.y}, k0 + kk, p, id,
+                                             live, warp_live);
+            }
+        }
+        // Every warp is done with this buffer (and knows whether any warp of
+        // the block is still live or has given up waiting).
+        const bool block_fault = __syncthreads_or(timed_out);
+        const bool block_live = __syncthreads_or(warp_live);
+        if (block_fault || !block_live) break;
+        if (leader && st + 2 < n_stages) {
+            dev::async_proxy_fence();
+            issue(st + 2);
+        }
     }
-    const double x = fma(p.x, t.cx, px * t.sx);
-    px = fma(px, t.cx, -p.x * t.sx);
-    const double y = fma(p.y, t.cy, py * t.sy);
-    py = fma(py, t.cy, -p.y * t.sy);
-    p.xx = x * x;
-    p.yy = y * y;
-    p.x = x;
-    p.px = px;
-    p.y = y;
-    p.py = py;
-    return fma(px, px, p.xx) + fma(py, py, p.yy);
-}
-
-template <bool OCT>
-__device__ __forceinline__ double turn_fast_rev(Particle &p, const Turn &t,
-                                                double mu) {
-    const double x = fma(p.x, t.cx, -p.px * t.sx);
-    double px = fma(p.x, t.sx, p.px * t.cx);
-    const double y = fma(p.y, t.cy, -p.py * t.sy);
-    double py = fma(p.y, t.sy, p.py * t.cy);
-    const double xx = x * x;
-    const double yy = y * y;
-    if (OCT) {
-        px = fma(-mu * x, fma(-3.0, yy, xx), px);
-        py = fma(-mu * y, fma(-3.0, xx, yy), py);
+    // A copy still in flight (issued for stage st + 1) must land before the
+    // block's shared memory is released.
+    if (st + 1 < n_stages && !timed_out) {
+        const uint32_t nx = st + 1;
+        if (!dev::mbar_wait(&full[nx & 1u], (nx >> 1) & 1u)) timed_out = true;
     }
-    px = px - (xx - yy);
-    py = fma(2.0 * x, y, py);
-    p.x = x;
-    p.px = px;
-    p.y = y;
-    p.py = py;
-    p.xx = xx;
-    p.yy = yy;
-    return fma(px, px, xx) + fma(py, py, yy);
-}
-
-template <int ARITH, bool OCT, bool REV>
-__device__ __forceinline__ double turn(Particle &p, const Turn &t, double mu) {
-    if (ARITH == HM_ARITH_EXACT)
-        return REV ? turn_exact_rev<OCT>(p, t, mu) : turn_exact_fwd<OCT>(p, t, mu);
-    return REV ? turn_fast_rev<OCT>(p, t, mu) : turn_fast_fwd<OCT>(p, t, mu);
-}
-
-// r < barrier^2 for r = +0, positive finite, +inf or NaN (r is a sum of
-// squares, never -0), as an unsigned 64-bit compare of the bit patterns:
-// non-negative doubles order like their bit patterns and every NaN pattern,
-// of either sign, lies above the pattern of +inf, so NaN/overflowed
-// particles are lost exactly when `(...) < barrier_pow_2` is false.  Keeps
-// the per-turn test off the FP64 pipe.
-__device__ __forceinline__ bool inside(double r, long long b2bits) {
-    return static_cast<unsigned long long>(__double_as_longlong(r)) <
-           static_cast<unsigned long long>(b2bits);
+    const bool fault = __syncthreads_or(timed_out);
+    if (fault && leader && c.fault) atomicOr(c.fault, 1u);
+    return !fault;
 }
 
 // One chunk of turns for the particles of one block (K per thread).
-template <int ARITH, bool OCT, bool REV, int K>
+template <int ARITH, bool OCT, bool REV, int K, bool STAGED>
 __global__ void __launch_bounds__(256)
 track_chunk_kernel(const TrackChunk c) {
     const uint32_t n_in = c.in_count ? *c.in_count : c.n_user;
@@ -221,50 +196,18 @@ track_chunk_kernel(const TrackChunk c) {
                 live[j] = !(isnan(x) || isnan(px) || isnan(y) || isnan(py));
             }
         }
-        p[j] = Particle{x, px, y, py, Rn::mul(x, x), Rn::mul(y, y)};
+        p[j] = dev::make_particle(x, px, y, py);
     }
 
-    const double mu = c.mu;
-    const long long b2 = c.b2bits;
-    const uint32_t nt = c.n_turns;
-    Turn t = nt ? load_turn(c.table, REV ? c.turn0 - 1u : c.turn0) : Turn{0.0, 0.0, 0.0, 0.0};
+    const Barrier bar = dev::make_barrier<ARITH>(c.b2bits);
     bool thread_live = false;
 #pragma unroll
     for (int j = 0; j < K; ++j) thread_live |= live[j];
-    bool warp_live = __any_sync(kFullMask, thread_live);
-    for (uint32_t k = 0; warp_live && k < nt; ++k) {
-        // Prefetch the next turn's record (clamped to this chunk).
-        const uint32_t kn = (k + 1 < nt) ? k + 1 : k;
-        const Turn tn = load_turn(c.table, REV ? c.turn0 - 1u - kn : c.turn0 + kn);
-        bool lost[K];
-        bool any_lost = false;
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            const double r = turn<ARITH, OCT, REV>(p[j], t, mu);
-            lost[j] = live[j] && !inside(r, b2);
-            any_lost |= lost[j];
-        }
-        if (__any_sync(kFullMask, any_lost)) {
-            // Rare path: freeze lost particles (set_to_nan, :123-129); their
-            // steps count the turns survived so far.
-            const uint32_t s = REV ? c.turn0 - k : c.turn0 + k;
-            bool any_live = false;
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                if (lost[j]) {
-                    const uint32_t i = id[j];
-                    c.ux[i] = quiet_nan();
-                    c.upx[i] = quiet_nan();
-                    c.uy[i] = quiet_nan();
-                    c.upy[i] = quiet_nan();
-                    c.usteps[i] = s;
-                    live[j] = false;
-                }
-                any_live |= live[j];
-            }
-            warp_live = __any_sync(kFullMask, any_live);
-        }
-        t = tn;
+    const bool warp_live = __any_sync(kFullMask, thread_live);
+    if (STAGED) {
+        if (!turns_staged<ARITH, OCT, REV, K>(c, bar, p, id, live, warp_live)) return;
+    } else {
+        turns_direct<ARITH, OCT, REV, K>(c, bar, p, id, live, warp_live);
     }
 
     if (c.out_idx == nullptr) {
@@ -304,6 +247,17 @@ track_chunk_kernel(const TrackChunk c) {
     }
 }
 
+template <int ARITH, bool OCT, bool REV, int K>
+cudaError_t launch_s(const TrackChunk &c, unsigned blocks, int threads, cudaStream_t s) {
+    if (c.stage_turns == 0) {
+        track_chunk_kernel<ARITH, OCT, REV, K, false><<<blocks, threads, 0, s>>>(c);
+    } else {
+        const size_t smem = size_t(c.stage_turns) * 2u * 32u;
+        track_chunk_kernel<ARITH, OCT, REV, K, true><<<blocks, threads, smem, s>>>(c);
+    }
+    return cudaGetLastError();
+}
+
 template <int ARITH, bool OCT, bool REV>
 cudaError_t launch_k(const TrackChunk &c, const TrackLaunch &l, uint32_t n_upper,
                      cudaStream_t s) {
@@ -313,12 +267,11 @@ cudaError_t launch_k(const TrackChunk &c, const TrackLaunch &l, uint32_t n_upper
     const unsigned blocks = unsigned((uint64_t(n_upper) + per_block - 1) / per_block);
     if (blocks == 0) return cudaSuccess;
     switch (K) {
-        case 1: track_chunk_kernel<ARITH, OCT, REV, 1><<<blocks, threads, 0, s>>>(c); break;
-        case 2: track_chunk_kernel<ARITH, OCT, REV, 2><<<blocks, threads, 0, s>>>(c); break;
-        case 4: track_chunk_kernel<ARITH, OCT, REV, 4><<<blocks, threads, 0, s>>>(c); break;
+        case 1: return launch_s<ARITH, OCT, REV, 1>(c, blocks, threads, s);
+        case 2: return launch_s<ARITH, OCT, REV, 2>(c, blocks, threads, s);
+        case 4: return launch_s<ARITH, OCT, REV, 4>(c, blocks, threads, s);
         default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 template <int ARITH>

@@ -27,50 +27,6 @@ namespace {
 
 using dev::Rn;
 
-__device__ __forceinline__ bool inside(double r, long long b2bits) {
-    return static_cast<unsigned long long>(__double_as_longlong(r)) <
-           static_cast<unsigned long long>(b2bits);
-}
-
-template <int ARITH, bool OCT>
-__device__ __forceinline__ double map_turn(double &x, double &px, double &y, double &py,
-                                           const dev::Turn &t, double mu) {
-    if (ARITH == HM_ARITH_EXACT) {
-        const double xx = Rn::mul(x, x), yy = Rn::mul(y, y);
-        double npx = Rn::add(px, Rn::sub(xx, yy));
-        double npy = Rn::add(py, Rn::mul(Rn::mul(-2.0, x), y));
-        if (OCT) {
-            npx = Rn::add(npx, Rn::mul(mu, Rn::sub(Rn::mul(xx, x), Rn::mul(Rn::mul(Rn::mul(3.0, y), y), x))));
-            npy = Rn::add(npy, Rn::mul(mu, Rn::sub(Rn::mul(yy, y), Rn::mul(Rn::mul(Rn::mul(3.0, x), x), y))));
-        }
-        const double nx = Rn::add(Rn::mul(x, t.cx), Rn::mul(npx, t.sx));
-        npx = Rn::add(Rn::mul(-x, t.sx), Rn::mul(npx, t.cx));
-        const double ny = Rn::add(Rn::mul(y, t.cy), Rn::mul(npy, t.sy));
-        npy = Rn::add(Rn::mul(-y, t.sy), Rn::mul(npy, t.cy));
-        x = nx;
-        px = npx;
-        y = ny;
-        py = npy;
-        return Rn::add(Rn::add(Rn::mul(x, x), Rn::mul(px, px)), Rn::add(Rn::mul(y, y), Rn::mul(py, py)));
-    }
-    const double xx = x * x, yy = y * y;
-    double npx = px + (xx - yy);
-    double npy = fma(-2.0 * x, y, py);
-    if (OCT) {
-        npx = fma(mu * x, fma(-3.0, yy, xx), npx);
-        npy = fma(mu * y, fma(-3.0, xx, yy), npy);
-    }
-    const double nx = fma(x, t.cx, npx * t.sx);
-    npx = fma(npx, t.cx, -x * t.sx);
-    const double ny = fma(y, t.cy, npy * t.sy);
-    npy = fma(npy, t.cy, -y * t.sy);
-    x = nx;
-    px = npx;
-    y = ny;
-    py = npy;
-    return fma(px, px, x * x) + fma(py, py, y * y);
-}
-
 template <int ARITH, bool OCT>
 __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -83,11 +39,17 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     a.opx[i] = px;
     a.oy[i] = y;
     a.opy[i] = py;
+    dev::Particle p = dev::make_particle(x, px, y, py);
+    const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     for (uint32_t k = 0; k < a.n_turns; ++k) {
         if (alive) {
-            const double r = map_turn<ARITH, OCT>(x, px, y, py, dev::load_turn(a.table, a.live_step + k), a.mu);
-            if (inside(r, a.b2bits)) {
+            const double r = dev::turn<ARITH, OCT, false>(p, dev::load_turn(a.table, a.live_step + k), a.mu);
+            if (dev::inside<ARITH>(r, p, bar)) {
                 steps += 1u;
+                x = p.x;
+                px = p.px;
+                y = p.y;
+                py = p.py;
             } else {
                 x = px = y = py = dev::quiet_nan();
                 alive = false;

@@ -104,6 +104,17 @@ hm_status hm_set_track_config(int threads, int per_thread, uint32_t chunk0,
                               uint32_t chunk_max);
 hm_status hm_get_track_config(int *threads, int *per_thread,
                               uint32_t *chunk0, uint32_t *chunk_max);
+/* How the tracking kernels read the per-turn records {sin wx, cos wx,
+ * sin wy, cos wy}: 0 = straight from global memory (a broadcast load per
+ * warp and turn); otherwise one thread per block brings stage_turns turns
+ * of records at a time into shared memory with a bulk copy (TMA,
+ * double-buffered, bounded waits) and every warp reads them from there.
+ * stage_turns is 0 or a power of two in [16, 512] (default 256); runs of
+ * one chunk use direct reads.  Process-wide; results do not depend on it.
+ * A staged copy that does not land within its bounded wait makes the call
+ * return HM_ERR_TIMEOUT. */
+hm_status hm_set_track_staging(uint32_t stage_turns);
+hm_status hm_get_track_staging(uint32_t *stage_turns);
 
 /* ---- host numerics ----------------------------------------------------- */
 

@@ -74,3 +74,30 @@ def gpu():
     lib = _capi.load()
     assert lib.hm_device_count() > 0, "no CUDA device visible to libhenon_b200"
     return lib
+
+
+def edge_barriers(x, px, y, py, n_turns, eps, mu, n_particles=4, spread=3):
+    """Barriers whose square lies within a few representable doubles of the
+    largest radius (x*x + px*px) + (y*y + py*py) some particles reach in
+    n_turns turns: their loss turn hangs on the last bit of that separately
+    rounded sum.  Returns (barriers, index of the particle each targets,
+    largest radius of every particle)."""
+    from oracle import oracle as O
+
+    tabs = O.tables(n_turns, *TUNES, "sps", epsilon=eps)
+    st = (x, px, y, py, np.zeros(x.size, np.uint32))
+    rmax = np.zeros(x.size)
+    with np.errstate(all="ignore"):
+        for _ in range(n_turns):
+            st = O.track(*st, tabs, 1, mu, 1e200)
+            r = (st[0] * st[0] + st[1] * st[1]) + (st[2] * st[2] + st[3] * st[3])
+            rmax = np.fmax(rmax, r)
+    ok = np.flatnonzero(np.isfinite(rmax) & (rmax > 0.05) & (rmax < 50.0))
+    picks = ok[np.linspace(0, ok.size - 1, n_particles).astype(int)]
+    out, who = [], []
+    for i in picks:
+        b = np.sqrt(rmax[i])
+        for d in range(-spread, spread + 1):
+            out.append(float(b + d * np.spacing(b)))
+            who.append(int(i))
+    return out, who, rmax

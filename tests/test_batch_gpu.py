@@ -67,3 +67,29 @@ def test_batch_graph_replays_identically(gpu):
         length = min(2 * length, 512)
         chunks += 1
     assert b.n_chunks() == chunks
+
+
+@pytest.mark.parametrize("arith", [0, 1])
+def test_batch_barriers_at_the_last_bit(gpu, arith):
+    # One set per barrier whose square lies within a few doubles of some
+    # particle's largest radius: each set's loss decisions must be those of
+    # a plain hm_track with that barrier (and, exact, of the oracle).
+    from conftest import TUNES, edge_barriers, grid
+    from oracle import oracle as O
+
+    x, px, y, py = grid(0.5, 8)
+    n_turns, eps, mu = 300, 16.0, 0.2
+    barriers, _, _ = edge_barriers(x, px, y, py, n_turns, eps, mu)
+    sets = [dict(omega_x=TUNES[0], omega_y=TUNES[1], epsilon=eps, mu=mu, n_particles=x.size,
+                 n_turns=n_turns, barrier=b) for b in barriers]
+    coords = tuple(np.tile(c, len(sets)) for c in (x, px, y, py))
+    res = sweep.run_sweep(sets, coords, arith=arith, chunk0=64, chunk_max=128)
+    tabs = O.tables(n_turns, *TUNES, "sps", epsilon=eps)
+    for s, r in zip(sets, res):
+        want = plain(s, x, px, y, py, arith)
+        np.testing.assert_array_equal(r["steps"], want[4])
+        for k, w in zip(("x", "px", "y", "py"), want[:4]):
+            assert_bitwise(r[k], w, k)
+        if arith == 0:
+            o = O.track(x, px, y, py, np.zeros(x.size, np.uint32), tabs, n_turns, mu, s["barrier"])
+            np.testing.assert_array_equal(r["steps"], o[4])

@@ -104,6 +104,19 @@ def test_track_config_roundtrip():
         C.set_track_config(*saved)
 
 
+def test_track_staging_roundtrip_and_validation():
+    saved = C.get_track_staging()
+    try:
+        for ok in (0, 16, 128, 512):
+            C.set_track_staging(ok)
+            assert C.get_track_staging() == ok
+        for bad in (1, 8, 48, 1024):
+            with pytest.raises(C.HMError):
+                C.set_track_staging(bad)
+    finally:
+        C.set_track_staging(saved)
+
+
 def test_workspace_size_is_linear():
     lib = C.load()
     a = lib.hm_track_workspace_bytes(1000)

@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import NAN, TUNES, assert_bitwise, golden_npz, grid
+from conftest import NAN, TUNES, assert_bitwise, edge_barriers, golden_npz, grid
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -71,6 +71,25 @@ def test_c1_full_size_exact(gpu):
         assert_bitwise(a, b)
 
 
+def test_barrier_decided_at_the_last_bit(gpu):
+    # For each target particle some of the barriers keep it for the whole
+    # run and some lose it at the turn of its largest radius; the GPU's
+    # decision must be the oracle's in every case.
+    x, px, y, py = grid(0.5, 8)
+    n_turns, eps, mu = 300, 16.0, 0.2
+    barriers, who, rmax = edge_barriers(x, px, y, py, n_turns, eps, mu)
+    kept = {i: set() for i in who}
+    for b, i in zip(barriers, who):
+        got, _, _ = run_gpu(x, px, y, py, n_turns, eps, mu, barrier=b)
+        want = run_oracle(x, px, y, py, n_turns, eps, mu, barrier=b)
+        np.testing.assert_array_equal(got[4], want[4], err_msg=f"barrier {b!r}")
+        for a, w in zip(got[:4], want[:4]):
+            assert_bitwise(a, w, f"barrier {b!r}")
+        kept[i].add(bool(want[4][i] == n_turns))
+        assert (want[4][i] == n_turns) == (rmax[i] < b * b)
+    assert all(v == {True, False} for v in kept.values())
+
+
 def test_split_calls_equal_one_call(gpu):
     x, px, y, py = grid(0.6, 32)
     one, _, _ = run_gpu(x, px, y, py, 3000, 16.0, 0.2)
@@ -93,6 +112,38 @@ def test_launch_shape_does_not_change_results(gpu):
                 assert_bitwise(a, b, str(cfg))
     finally:
         C.set_track_config(*saved)
+
+
+@pytest.mark.parametrize("stage", [16, 128, 512])
+def test_staged_turn_records_give_identical_results(gpu, stage):
+    # Turn records brought into shared memory by bulk copies, stage by
+    # stage: chunk lengths that are not multiples of the stage, one to four
+    # particles per thread, forward and reverse.
+    x, px, y, py = grid(0.6, 40)
+    ref = run_oracle(x, px, y, py, 2500, 64.0, 0.2)
+    saved, saved_stage = C.get_track_config(), C.get_track_staging()
+    try:
+        C.set_track_staging(stage)
+        assert C.get_track_staging() == stage
+        for cfg in [(32, 1, 64, 64), (128, 2, 100, 700), (256, 4, 512, 16384)]:
+            C.set_track_config(*cfg)
+            got, _, _ = run_gpu(x, px, y, py, 2500, 64.0, 0.2)
+            np.testing.assert_array_equal(got[4], ref[4], err_msg=str(cfg))
+            for a, b in zip(got[:4], ref[:4]):
+                assert_bitwise(a, b, str(cfg))
+        C.set_track_config(128, 2, 300, 300)
+        g = golden_npz("ref_reverse.npz")
+        t = C.Tracker(1000, TUNES[0], TUNES[1], "sps", NAN, 64.0, 0)
+        p = C.Particles(g["x0"], g["px0"], g["y0"], g["py0"])
+        t.track(p, 1000, 0.1, 10.0)
+        t.track(p, 1000, 0.1, 10.0, NAN, True)
+        x1, px1, y1, py1, s1 = p.state()
+        for a, k in zip((x1, px1, y1, py1), ("bx", "bpx", "by", "bpy")):
+            assert_bitwise(a, g[k], k)
+        np.testing.assert_array_equal(s1, g["bsteps"])
+    finally:
+        C.set_track_config(*saved)
+        C.set_track_staging(saved_stage)
 
 
 def test_reverse_matches_reference_fixture(gpu):
