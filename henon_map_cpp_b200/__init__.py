@@ -69,6 +69,17 @@ class particles:
     def reset(self):
         self.particles.reset()
 
+    @property
+    def kick_seed(self):
+        """Key of the reproducible random kicks of henon_tracker.track
+        (kick_module not NaN): the kick of a particle at a turn is a
+        function of (kick_seed, particle index, turn)."""
+        return self.particles.kick_seed
+
+    @kick_seed.setter
+    def kick_seed(self, seed):
+        self.particles.kick_seed = int(seed)
+
     def add_ghost(self, module, displacement_kind):
         self.particles.add_ghost(module, displacement_kind)
 

@@ -89,6 +89,8 @@ _SIGNATURES = {
     "hm_particles_device_ptr": (None, [c_void_p, c_int, POINTER(c_void_p)]),
     "hm_particles_observable": (None, [c_void_p, c_int, _PD]),
     "hm_track": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, c_double, c_int]),
+    "hm_particles_set_kick_seed": (None, [c_void_p, ctypes.c_uint64]),
+    "hm_particles_get_kick_seed": (None, [c_void_p, POINTER(ctypes.c_uint64)]),
     "hm_track_workspace_bytes": (c_size_t, [c_size_t]),
     "hm_track_device": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
                                c_void_p, c_uint64, c_uint32, c_uint32, c_double, c_double, c_int,
@@ -330,6 +332,17 @@ class Particles:
         v = c_uint32()
         call("hm_particles_global_steps", self.h, ctypes.byref(v))
         return int(v.value)
+
+    @property
+    def kick_seed(self) -> int:
+        """Key of the reproducible random kicks of track(kick_module=...)."""
+        v = ctypes.c_uint64()
+        call("hm_particles_get_kick_seed", self.h, ctypes.byref(v))
+        return int(v.value)
+
+    @kick_seed.setter
+    def kick_seed(self, seed: int) -> None:
+        call("hm_particles_set_kick_seed", self.h, ctypes.c_uint64(int(seed)))
 
     def get(self, field: int) -> np.ndarray:
         out = np.empty(self.n_total, dtype=FIELD_DTYPE[field])

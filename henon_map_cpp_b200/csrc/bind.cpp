@@ -317,6 +317,16 @@ PYBIND11_MODULE(henon_map_engine, m) {
                       const std::vector<double> &, const std::vector<double> &>(),
              py::arg("x"), py::arg("px"), py::arg("y"), py::arg("py"))
         .def("reset", [](Particles &p) { check(hm_particles_reset(p.h)); })
+        // Key of the reproducible random kicks of track(kick_module=...);
+        // no counterpart in the reference, whose kicks are clock()-seeded.
+        .def_property(
+            "kick_seed",
+            [](const Particles &p) {
+                uint64_t v = 0;
+                check(hm_particles_get_kick_seed(p.h, &v));
+                return v;
+            },
+            [](Particles &p, uint64_t v) { check(hm_particles_set_kick_seed(p.h, v)); })
         .def("add_ghost", [](Particles &p, double module, const std::string &dir) {
             check(hm_particles_add_ghost(p.h, module, dir.c_str()));
         }, py::arg("displacement_module"), py::arg("direction"))

@@ -178,7 +178,7 @@ hm_status track_driver(double *x, double *px, double *y, double *py,
                        uint64_t table_len, uint32_t s0, uint32_t n_turns,
                        double mu, double barrier, bool inverse, hm_arith arith,
                        void *workspace, cudaStream_t stream,
-                       uint32_t *turns_done) {
+                       uint32_t *turns_done, double kick_module, unsigned long long kick_seed) {
     *turns_done = 0;
     if (n == 0 || n_turns == 0) {
         *turns_done = n_turns;  // nothing to move; the turn counter still advances
@@ -210,6 +210,8 @@ hm_status track_driver(double *x, double *px, double *y, double *py,
     c.table = table;
     c.mu = mu;
     c.b2bits = b2bits;
+    c.kick_module = kick_module;
+    c.kick_seed = kick_seed;
     TrackLaunch l{int(arith), mu != 0.0, inverse, cfg.per_thread, cfg.threads};
 
     const bool one_chunk = n_turns <= cfg.chunk0;
@@ -703,6 +705,18 @@ hm_status hm_particles_observable(const hm_particles *p, hm_observable kind, dou
     return ok();
 }
 
+hm_status hm_particles_set_kick_seed(hm_particles *p, uint64_t seed) {
+    if (!p) return fail(HM_ERR_INVALID_ARG, "null particles");
+    p->kick_seed = seed;
+    return ok();
+}
+
+hm_status hm_particles_get_kick_seed(const hm_particles *p, uint64_t *seed) {
+    if (!p || !seed) return fail(HM_ERR_INVALID_ARG, "null particles or output");
+    *seed = p->kick_seed;
+    return ok();
+}
+
 // ---- tracking ---------------------------------------------------------------------
 
 size_t hm_track_workspace_bytes(size_t n) { return hm::track_workspace_bytes(n); }
@@ -727,8 +741,6 @@ hm_status hm_track(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu, 
         if (uint64_t(n_turns) + p->global_steps > t->allowed_steps)
             return fail(HM_ERR_BUDGET, "The number of turns is too large.");
     }
-    if (!std::isnan(kick_module))
-        return fail(HM_ERR_NOT_SUPPORTED, "random kicks (kick_module) are not provided by this build");
     if (inverse && n_turns > p->live_step)
         return fail(HM_ERR_BUDGET,
                     "The number of turns is too large. (inverse tracking past the particles' steps)");
@@ -741,7 +753,8 @@ hm_status hm_track(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu, 
     const hm_status s = hm::track_driver(
         p->x.as<double>(), p->px.as<double>(), p->y.as<double>(), p->py.as<double>(),
         p->steps.as<uint32_t>(), p->n_total, t->table.as<const double>(), t->allowed_steps,
-        p->live_step, n_turns, mu, barrier, inverse != 0, t->arith, ws, 0, &done);
+        p->live_step, n_turns, mu, barrier, inverse != 0, t->arith, ws, 0, &done, kick_module,
+        p->kick_seed);
     if (s != HM_OK && s != HM_ERR_CANCELLED) return s;
     // global_steps follows the turns applied (src/henon.cu:3181-3184).
     if (inverse) {

@@ -221,6 +221,99 @@ __device__ __forceinline__ double turn(Particle &p, const Turn &t, double mu) {
     return REV ? turn_fast_rev<OCT>(p, t, mu) : turn_fast_fwd<OCT>(p, t, mu);
 }
 
+// ---- reproducible random kicks ---------------------------------------------------
+// The reference kicks a particle by kick_module along a random direction
+// before the sextupole (random_4d_kick, src/henon.cu:387-405, from a
+// clock()-seeded curand stream).  Here the direction comes from a
+// counter-based generator keyed by (seed, particle index, table index of
+// the turn): the same run gives the same kicks however it is split into
+// launches, chunks and compacted lists.
+//   Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+//   easy as 1, 2, 3", SC'11): counter {turn, attempt, idx_lo, idx_hi}, key
+//   {seed_lo, seed_hi}.
+//   Direction uniform on the unit 3-sphere by Marsaglia's method (Ann. Math.
+//   Statist. 43 (1972) 645-646): (u1, u2), (u3, u4) uniform in the unit
+//   disc, s1 = u1^2+u2^2, s2 = u3^2+u4^2, direction (u1, u2, u3 f, u4 f),
+//   f = sqrt((1 - s1) / s2).
+// One Philox block gives a candidate point for each disc
+// (u = (int32(r) + 0.5) * 2^-31, exact); each disc keeps its first
+// accepted point.  After kKickAttempts attempts (probability < 1e-42) a
+// disc without a point takes (0, 0) (first) or (1, 0) (second).  Every
+// operation is a correctly rounded IEEE one, so a host restatement gives
+// the same bits.
+constexpr uint32_t kKickAttempts = 64u;
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ double kick_uniform(uint32_t r) {
+    return Rn::mul(Rn::add(double(int32_t(r)), 0.5), 0x1p-31);
+}
+
+struct KickDirection {
+    double d0, d1, d2, d3;
+};
+
+__device__ __forceinline__ KickDirection kick_direction(unsigned long long seed,
+                                                        unsigned long long idx, uint32_t turn) {
+    const uint32_t k0 = uint32_t(seed), k1 = uint32_t(seed >> 32);
+    double u1 = 0.0, u2 = 0.0, u3 = 1.0, u4 = 0.0, s1 = 0.0, s2 = 1.0;
+    bool got1 = false, got2 = false;
+    for (uint32_t a = 0; a < kKickAttempts && !(got1 && got2); ++a) {
+        const uint4 r = philox4x32_10(make_uint4(turn, a, uint32_t(idx), uint32_t(idx >> 32)), k0, k1);
+        if (!got1) {
+            const double a1 = kick_uniform(r.x), a2 = kick_uniform(r.y);
+            const double s = Rn::add(Rn::mul(a1, a1), Rn::mul(a2, a2));
+            if (s < 1.0) {
+                u1 = a1;
+                u2 = a2;
+                s1 = s;
+                got1 = true;
+            }
+        }
+        if (!got2) {
+            const double a3 = kick_uniform(r.z), a4 = kick_uniform(r.w);
+            const double s = Rn::add(Rn::mul(a3, a3), Rn::mul(a4, a4));
+            if (s < 1.0 && s > 0.0) {
+                u3 = a3;
+                u4 = a4;
+                s2 = s;
+                got2 = true;
+            }
+        }
+    }
+    const double f = __dsqrt_rn(Rn::div(Rn::sub(1.0, s1), s2));
+    return KickDirection{u1, u2, Rn::mul(u3, f), Rn::mul(u4, f)};
+}
+
+// Adds (forward) or subtracts (backward) the kick of module km along d and
+// refreshes the carried squares.
+template <bool SUB>
+__device__ __forceinline__ void apply_kick(Particle &p, const KickDirection &d, double km) {
+    if (SUB) {
+        p.x = Rn::sub(p.x, Rn::mul(d.d0, km));
+        p.px = Rn::sub(p.px, Rn::mul(d.d1, km));
+        p.y = Rn::sub(p.y, Rn::mul(d.d2, km));
+        p.py = Rn::sub(p.py, Rn::mul(d.d3, km));
+    } else {
+        p.x = Rn::add(p.x, Rn::mul(d.d0, km));
+        p.px = Rn::add(p.px, Rn::mul(d.d1, km));
+        p.y = Rn::add(p.y, Rn::mul(d.d2, km));
+        p.py = Rn::add(p.py, Rn::mul(d.d3, km));
+    }
+    p.xx = Rn::mul(p.x, p.x);
+    p.yy = Rn::mul(p.y, p.y);
+}
+
 // ---- the barrier test ------------------------------------------------------------
 // A particle is kept while r < barrier^2 (check_barrier, src/henon.cu:
 // 113-116).  r is a sum of squares, so it is +0, positive, +inf or NaN, and

@@ -91,6 +91,8 @@ struct hm_particles {
     // Generator of "random" ghost directions: default-seeded, one per
     // particle set, as the reference's particles_4d::rng.
     std::mt19937_64 rng;
+    // Key of the counter-based random kicks of hm_track (0 by default).
+    unsigned long long kick_seed = 0;
 };
 
 // Modulation tables on the device (henon_tracker_gpu, src/henon.h:212-228).
@@ -137,6 +139,10 @@ struct TrackChunk {
     // (a power of two in [16, 512]; needs a 16-byte aligned table).
     uint32_t stage_turns;
     uint32_t *fault;       // set to nonzero when a staged copy timed out
+    // Random kick of this module per turn (NaN: none), direction keyed by
+    // (kick_seed, caller's particle index, table index of the turn).
+    double kick_module;
+    unsigned long long kick_seed;
 };
 
 struct TrackLaunch {
@@ -162,12 +168,14 @@ constexpr size_t track_workspace_bytes(size_t n) {
 // Host driver of the chunked tracking launches (capi.cpp).  `workspace`
 // holds track_workspace_bytes(n) bytes of device memory (may be null when
 // n_turns fits one chunk); *turns_done receives the turns applied.
+// kick_module NaN means no random kicks.
 hm_status track_driver(double *x, double *px, double *y, double *py,
                        uint32_t *steps, size_t n, const double *table,
                        uint64_t table_len, uint32_t s0, uint32_t n_turns,
                        double mu, double barrier, bool inverse, hm_arith arith,
                        void *workspace, cudaStream_t stream,
-                       uint32_t *turns_done);
+                       uint32_t *turns_done, double kick_module = __builtin_nan(""),
+                       unsigned long long kick_seed = 0ull);
 
 // Elementwise observable kernel launcher.
 cudaError_t launch_observable(const double *x, const double *px,

@@ -204,9 +204,19 @@ hm_status hm_tracker_tangent_matrices(const hm_tracker *t,
 
 /* henon_tracker_gpu::track, src/henon.cu:3155-3185: n_turns turns of the
  * map on every particle, fused into chunked multi-turn launches.
- * kick_module must be NaN (random kicks are not provided). */
+ * kick_module not NaN: every turn first kicks each particle by kick_module
+ * along a random direction (random_4d_kick, src/henon.cu:387-405).  Unlike
+ * the reference's clock()-seeded stream, the direction is a function of
+ * (the particles' kick seed, particle index, table index of the turn):
+ * Philox4x32-10 and Marsaglia's uniform point on the 3-sphere, so a run is
+ * reproducible and independent of launch shape and chunking.  Backward
+ * turns subtract the kick of the same table index after the inverse
+ * sextupole, undoing the forward turn's kick. */
 hm_status hm_track(hm_tracker *t, hm_particles *p, uint32_t n_turns,
                    double mu, double barrier, double kick_module, int inverse);
+/* Key of the kicks of hm_track for these particles (0 after creation). */
+hm_status hm_particles_set_kick_seed(hm_particles *p, uint64_t seed);
+hm_status hm_particles_get_kick_seed(const hm_particles *p, uint64_t *seed);
 
 /* Kernel-level form of the same operation on caller-owned device arrays
  * (the loop body of gpu_henon_track, src/henon.cu:636-691).  start_step is

@@ -127,6 +127,140 @@ static void turn(double *x, double *px, double *y, double *py, uint32_t *steps,
     }
 }
 
+/* ---- reproducible random kicks --------------------------------------------
+ * The reference kicks every particle by kick_module along a random direction
+ * before the sextupole (random_4d_kick, src/henon.cu:362-405, called from
+ * henon_step :438-441 and :465-468 in reverse), from a clock()-seeded curand
+ * stream on the GPU.  This library draws the direction from a counter-based
+ * generator keyed by (seed, particle index, table index of the turn), so
+ * that a run is reproducible and independent of how it is split into
+ * launches.  The restatement here is bit-identical to the device code:
+ *   Philox4x32-10 (J. K. Salmon, M. A. Moraes, R. O. Dror, D. E. Shaw,
+ *   "Parallel random numbers: as easy as 1, 2, 3", SC'11): counter
+ *   {turn, attempt, idx_lo, idx_hi}, key {seed_lo, seed_hi};
+ *   a direction uniform on the unit 3-sphere by Marsaglia's method
+ *   (Ann. Math. Statist. 43 (1972) 645-646): (u1, u2) and (u3, u4) uniform
+ *   in the unit disc, s1 = u1^2+u2^2, s2 = u3^2+u4^2, then
+ *   (u1, u2, u3 f, u4 f) with f = sqrt((1 - s1) / s2).
+ * Each attempt turns one Philox block into candidate points for both discs
+ * (u = (int32(r) + 0.5) * 2^-31, exact); a disc keeps its first accepted
+ * point.  After 64 attempts (probability of getting there < 1e-42) a disc
+ * without a point takes (0, 0) for the first disc and (1, 0) for the
+ * second. */
+void or_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+static double kick_uniform(uint32_t r) { return ((double)(int32_t)r + 0.5) * 0x1p-31; }
+
+void or_kick_direction(uint64_t seed, uint64_t idx, uint32_t turn, double d[4]) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    double u1 = 0.0, u2 = 0.0, u3 = 1.0, u4 = 0.0, s1 = 0.0, s2 = 1.0;
+    int got1 = 0, got2 = 0;
+    for (uint32_t a = 0; a < 64u && !(got1 && got2); ++a) {
+        const uint32_t ctr[4] = {turn, a, (uint32_t)idx, (uint32_t)(idx >> 32)};
+        uint32_t r[4];
+        or_philox4x32_10(ctr, key, r);
+        if (!got1) {
+            const double a1 = kick_uniform(r[0]), a2 = kick_uniform(r[1]);
+            const double s = a1 * a1 + a2 * a2;
+            if (s < 1.0) {
+                u1 = a1;
+                u2 = a2;
+                s1 = s;
+                got1 = 1;
+            }
+        }
+        if (!got2) {
+            const double a3 = kick_uniform(r[2]), a4 = kick_uniform(r[3]);
+            const double s = a3 * a3 + a4 * a4;
+            if (s < 1.0 && s > 0.0) {
+                u3 = a3;
+                u4 = a4;
+                s2 = s;
+                got2 = 1;
+            }
+        }
+    }
+    const double f = sqrt((1.0 - s1) / s2);
+    d[0] = u1;
+    d[1] = u2;
+    d[2] = u3 * f;
+    d[3] = u4 * f;
+}
+
+/* One turn with a kick of module km along the direction of (seed, j, table
+ * index): added before the sextupole going forward; going backward,
+ * subtracted after the inverse sextupole (undoing the forward turn's kick),
+ * then the barrier test. */
+static void turn_kicked(double *x, double *px, double *y, double *py, uint32_t *steps,
+                        const double *sinx, const double *cosx, const double *siny,
+                        const double *cosy, double barrier_pow_2, double mu, int reverse,
+                        double km, uint64_t seed, uint64_t j) {
+    if (is_lost(*x, *px, *y, *py)) return;
+    double d[4];
+    if (!reverse) {
+        or_kick_direction(seed, j, *steps, d);
+        *x += d[0] * km;
+        *px += d[1] * km;
+        *y += d[2] * km;
+        *py += d[3] * km;
+        turn(x, px, y, py, steps, sinx, cosx, siny, cosy, barrier_pow_2, mu, 0);
+        return;
+    }
+    or_kick_direction(seed, j, *steps - 1, d);
+    /* the inverse turn without its barrier test (an overflowed state is
+     * lost either way), then the kick, then the test */
+    turn(x, px, y, py, steps, sinx, cosx, siny, cosy, INFINITY, mu, 1);
+    if (is_lost(*x, *px, *y, *py)) return;
+    *x -= d[0] * km;
+    *px -= d[1] * km;
+    *y -= d[2] * km;
+    *py -= d[3] * km;
+    const double X = *x, PX = *px, Y = *y, PY = *py;
+    if (!((X * X + PX * PX) + (Y * Y + PY * PY) < barrier_pow_2)) {
+        *steps += 1u; /* the inverse turn counted a step that was not survived */
+        *x = NAN;
+        *px = NAN;
+        *y = NAN;
+        *py = NAN;
+    }
+}
+
+/* henon_tracker::track with random kicks (kick_module not NaN). */
+void or_track_kicked(double *x, double *px, double *y, double *py, uint32_t *steps, size_t n,
+                     const double *sinx, const double *cosx, const double *siny,
+                     const double *cosy, uint32_t n_turns, double mu, double barrier,
+                     int reverse, double kick_module, uint64_t seed, int n_threads) {
+    const double b2 = barrier * barrier;
+#ifdef _OPENMP
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(n_threads)
+#endif
+    for (long long j = 0; j < (long long)n; ++j)
+        for (uint32_t k = 0; k < n_turns; ++k)
+            turn_kicked(&x[j], &px[j], &y[j], &py[j], &steps[j], sinx, cosx, siny, cosy, b2, mu,
+                        reverse, kick_module, seed, (uint64_t)j);
+    (void)n_threads;
+}
+
 /* henon_tracker::track (src/henon.cu:2701-2752): n_turns turns of every
  * particle, particles spread over n_threads OpenMP threads (<=0: all). */
 void or_track(double *x, double *px, double *y, double *py, uint32_t *steps,

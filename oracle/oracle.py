@@ -59,6 +59,11 @@ def lib() -> ctypes.CDLL:
         L.or_max_threads.restype = ctypes.c_int
         L.or_tangent_matrix.argtypes = [_D] * 9 + [_PD]
         L.or_matmul4.argtypes = [_PD, _PD, _PD]
+        L.or_philox4x32_10.argtypes = [_PU32, _PU32, _PU32]
+        L.or_kick_direction.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, _PD]
+        L.or_track_kicked.argtypes = [_PD, _PD, _PD, _PD, _PU32, ctypes.c_size_t, _PD, _PD, _PD,
+                                      _PD, ctypes.c_uint32, _D, _D, ctypes.c_int, _D,
+                                      ctypes.c_uint64, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -129,6 +134,41 @@ def track(x, px, y, py, steps, tabs, n_turns: int, mu: float, barrier: float,
     lib().or_track(_p(x), _p(px), _p(y), _p(py), _p(steps, _PU32), x.size,
                    _p(sx), _p(cx), _p(sy), _p(cy), n_turns, mu, barrier,
                    int(bool(inverse)), int(n_threads))
+    return x, px, y, py, steps
+
+
+# ---- reproducible random kicks -------------------------------------------------------
+
+def philox4x32_10(ctr, key) -> np.ndarray:
+    """One Philox4x32-10 block (Salmon et al., SC'11) of a 4-word counter and
+    a 2-word key."""
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.empty(4, dtype=np.uint32)
+    lib().or_philox4x32_10(_p(c, _PU32), _p(k, _PU32), _p(out, _PU32))
+    return out
+
+
+def kick_direction(seed: int, idx: int, turn: int) -> np.ndarray:
+    """Unit 4-vector of the kick of particle idx at table index turn."""
+    out = np.empty(4)
+    lib().or_kick_direction(int(seed), int(idx), int(turn), _p(out))
+    return out
+
+
+def track_kicked(x, px, y, py, steps, tabs, n_turns: int, mu: float, barrier: float,
+                 kick_module: float, seed: int, inverse: bool = False, n_threads: int = 0):
+    """track with a kick of module kick_module per turn along the direction
+    of (seed, particle index, table index); returns (x, px, y, py, steps)."""
+    x = np.array(x, dtype=np.float64, copy=True)
+    px = np.array(px, dtype=np.float64, copy=True)
+    y = np.array(y, dtype=np.float64, copy=True)
+    py = np.array(py, dtype=np.float64, copy=True)
+    steps = np.array(steps, dtype=np.uint32, copy=True)
+    sx, cx, sy, cy = (np.ascontiguousarray(t, dtype=np.float64) for t in tabs)
+    lib().or_track_kicked(_p(x), _p(px), _p(y), _p(py), _p(steps, _PU32), x.size,
+                          _p(sx), _p(cx), _p(sy), _p(cy), n_turns, mu, barrier,
+                          int(bool(inverse)), kick_module, int(seed), int(n_threads))
     return x, px, y, py, steps
 
 

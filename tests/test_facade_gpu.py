@@ -183,3 +183,17 @@ def test_track_indicators_through_facade(gpu):
     assert_bitwise(mg.get_values(), mg2.get_values())
     assert_bitwise(np.asarray(tu.get_tune2_y()), np.asarray(tu2.get_tune2_y()))
     assert_bitwise(M.get_matrix(), M2.get_matrix())
+
+
+def test_kicked_track_through_facade(gpu):
+    x, px, y, py = grid(0.4, 12)
+    p = hm.particles(x, px, y, py)
+    assert p.kick_seed == 0
+    p.kick_seed = 2024
+    t = hm.henon_tracker(800, *TUNES, "sps", np.nan, 16.0, 0)
+    t.track(p, 800, 0.2, kick_module=5e-4)
+    want = O.track_kicked(x, px, y, py, np.zeros(x.size, np.uint32),
+                          O.tables(800, *TUNES, "sps", epsilon=16.0), 800, 0.2, 10.0, 5e-4, 2024)
+    np.testing.assert_array_equal(p.get_steps(), want[4])
+    assert_bitwise(p.get_x(), want[0])
+    assert_bitwise(p.get_py(), want[3])

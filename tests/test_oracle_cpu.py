@@ -146,3 +146,39 @@ def test_oracle_equals_reference_build_live(eps, mu, nt):
     for a, b in zip(got[:4], want[:4]):
         assert_bitwise(a, b)
     np.testing.assert_array_equal(got[4], want[4])
+
+
+def test_philox_known_answers():
+    # Philox4x32-10 known-answer vectors published with the generator
+    # (Random123 kat_vectors: counter, key -> output).
+    kat = [([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+           ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+           ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+            [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1])]
+    for ctr, key, want in kat:
+        np.testing.assert_array_equal(O.philox4x32_10(ctr, key), np.array(want, np.uint32))
+
+
+def test_kick_directions_are_unit_and_isotropic():
+    d = np.array([O.kick_direction(99, i, t) for i in range(2000) for t in (0, 1, 12345)])
+    np.testing.assert_allclose(np.einsum("ij,ij->i", d, d), 1.0, rtol=0, atol=1e-15)
+    assert np.abs(d.mean(axis=0)).max() < 0.02           # 6000 samples: sd 0.0065
+    cov = d.T @ d / len(d)
+    np.testing.assert_allclose(cov, np.eye(4) / 4, atol=0.015)
+    # a function of (seed, particle, turn) only
+    np.testing.assert_array_equal(O.kick_direction(99, 7, 3), O.kick_direction(99, 7, 3))
+    assert not np.array_equal(O.kick_direction(99, 7, 3), O.kick_direction(98, 7, 3))
+    assert not np.array_equal(O.kick_direction(99, 7, 3), O.kick_direction(99, 7, 4))
+
+
+def test_kicked_oracle_moves_each_turn_by_the_kick():
+    # With the rotation turned into the identity (omega = 0 tables) and a
+    # particle at the origin, one kicked turn leaves kick * direction plus
+    # the sextupole terms of that small displacement.
+    tabs = (np.zeros(3), np.ones(3), np.zeros(3), np.ones(3))
+    z = np.zeros(1)
+    got = O.track_kicked(z, z, z, z, np.zeros(1, np.uint32), tabs, 1, 0.0, 10.0, 1e-6, 5)
+    d = O.kick_direction(5, 0, 0)
+    assert got[4][0] == 1
+    np.testing.assert_allclose([got[0][0], got[2][0]], 1e-6 * d[[0, 2]], rtol=0, atol=1e-20)
+    np.testing.assert_allclose([got[1][0], got[3][0]], 1e-6 * d[[1, 3]], rtol=0, atol=1e-11)

@@ -146,6 +146,67 @@ def test_staged_turn_records_give_identical_results(gpu, stage):
         C.set_track_staging(saved_stage)
 
 
+def run_kicked(x, px, y, py, n_turns, eps, mu, kick, seed, arith=0, chunks=None):
+    t = C.Tracker(n_turns, TUNES[0], TUNES[1], "sps", NAN, eps, 0)
+    t.arith = arith
+    p = C.Particles(x, px, y, py)
+    p.kick_seed = seed
+    for n in (chunks or [n_turns]):
+        t.track(p, n, mu, 10.0, kick)
+    return p, t
+
+
+@pytest.mark.parametrize("mu", [0.0, 0.2])
+def test_kicked_tracking_matches_oracle(gpu, mu):
+    # Reproducible random kicks: bit-identical to the oracle's restatement
+    # (Philox4x32-10 + Marsaglia's point on the 3-sphere), independent of
+    # launch shape, staging and the split into calls.
+    x, px, y, py = grid(0.6, 24)
+    n_turns, eps, kick, seed = 3000, 16.0, 2e-3, 0x1234_5678_9ABC
+    tabs = O.tables(n_turns, *TUNES, "sps", epsilon=eps)
+    want = O.track_kicked(x, px, y, py, np.zeros(x.size, np.uint32), tabs, n_turns, mu, 10.0,
+                          kick, seed)
+    plain = O.track(x, px, y, py, np.zeros(x.size, np.uint32), tabs, n_turns, mu, 10.0)
+    assert not np.array_equal(want[4], plain[4]) or not np.array_equal(want[0], plain[0])
+    saved, saved_stage = C.get_track_config(), C.get_track_staging()
+    try:
+        for cfg, stage, chunks in [((128, 2, 512, 16384), 256, None),
+                                   ((64, 4, 100, 300), 0, [1, 999, 2000]),
+                                   ((256, 1, 64, 64), 16, [1500, 1500])]:
+            C.set_track_config(*cfg)
+            C.set_track_staging(stage)
+            p, _ = run_kicked(x, px, y, py, n_turns, eps, mu, kick, seed, chunks=chunks)
+            got = p.state()
+            np.testing.assert_array_equal(got[4], want[4], err_msg=str(cfg))
+            for a, b in zip(got[:4], want[:4]):
+                assert_bitwise(a, b, str(cfg))
+    finally:
+        C.set_track_config(*saved)
+        C.set_track_staging(saved_stage)
+    # another seed, other kicks
+    p2, _ = run_kicked(x, px, y, py, n_turns, eps, mu, kick, seed + 1)
+    assert not np.array_equal(p2.get(C.FIELD_X), want[0], equal_nan=True)
+
+
+def test_kicked_reverse_undoes_forward_kicks(gpu):
+    x, px, y, py = grid(0.3, 16)
+    n_turns, eps, mu, kick, seed = 1000, 8.0, 0.1, 1e-4, 77
+    p, t = run_kicked(x, px, y, py, n_turns, eps, mu, kick, seed)
+    tabs = O.tables(n_turns, *TUNES, "sps", epsilon=eps)
+    fwd = O.track_kicked(x, px, y, py, np.zeros(x.size, np.uint32), tabs, n_turns, mu, 10.0,
+                         kick, seed)
+    t.track(p, n_turns, mu, 10.0, kick, True)
+    back = O.track_kicked(*fwd, tabs, n_turns, mu, 10.0, kick, seed, inverse=True)
+    got = p.state()
+    np.testing.assert_array_equal(got[4], back[4])
+    for a, b in zip(got[:4], back[:4]):
+        assert_bitwise(a, b)
+    alive = ~np.isnan(got[0])
+    assert alive.sum() > x.size // 2
+    np.testing.assert_allclose(got[0][alive], x[alive], atol=1e-9)
+    np.testing.assert_allclose(got[1][alive], px[alive], atol=1e-9)
+
+
 def test_reverse_matches_reference_fixture(gpu):
     g = golden_npz("ref_reverse.npz")
     t = C.Tracker(1000, TUNES[0], TUNES[1], "sps", NAN, 64.0, 0)
@@ -191,8 +252,6 @@ def test_budget_errors_keep_reference_messages(gpu):
         t.track(p, 41, 0.0, 10.0)
     with pytest.raises(C.HMError, match="The number of turns is too large."):
         t.track(p, 61, 0.0, 10.0, NAN, True)
-    with pytest.raises(NotImplementedError):
-        t.track(p, 1, 0.0, 10.0, 1e-3)
     assert p.global_steps == 60
     with pytest.raises(C.HMError, match="Unknown modulation kind"):
         C.Tracker(10, 0.1, 0.2, "nope")
