@@ -49,6 +49,10 @@ MUS = (0.0, 0.2)
 BARRIER = 10.0
 FLOPS_PER_TURN = {False: 26.0, True: 42.0}  # mu == 0 / mu != 0 (algorithmic)
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per particle of a tracking launch's input list,
+# measured by ncu on the staged exact kernel (512x512 DA scan, 1024-turn
+# chunk of 262,144 particles: 8.42 MB read, 0.3 KB written).
+NCU_BYTES_PER_LIST_PARTICLE = 32.1
 
 
 def parse_args():
@@ -64,6 +68,12 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched / adjoint / indicator measurements")
+    ap.add_argument("--only", choices=["batched", "adjoint", "indicators", "tunes"], default=None,
+                    help="run one supplementary measurement alone and print its JSON")
+    ap.add_argument("--extra-side", type=int, default=None,
+                    help="grid side of --only indicators / tunes (default 512 / 128)")
+    ap.add_argument("--extra-turns", type=int, default=None,
+                    help="turns of --only indicators / tunes (default 1e5 / 1e4)")
     ap.add_argument("--stage-turns", type=int, default=None,
                     help="turn records per staged bulk copy (0: direct reads; "
                          "default: the library's setting)")
@@ -207,7 +217,7 @@ def bench_batched(C, arith):
 
     sets, coords = sweep.heterogeneous_sets(seed=20261203)
     b = C.Batch(sets)
-    b.configure(arith, 2, 512, 16384)
+    b.configure(arith, 1, 512, 16384)
     b.load(*coords)
     b.run(True)  # capture + warm-up
     times = []
@@ -217,6 +227,13 @@ def bench_batched(C, arith):
         times.append(time.perf_counter() - t0)
     t_batch = min(times)
     steps_batch = b.get(C.FIELD_STEPS)
+    # the same batch tracked as one group (no overlap of chunk ramp-downs)
+    b.set_groups(1)
+    b.run(True)
+    t0 = time.perf_counter()
+    b.run(True)
+    t_one_group = time.perf_counter() - t0
+    b.set_groups(4)
     # plain: one chunked tracking call per set on device arrays
     t_plain, equal, o = 0.0, True, 0
     stream = torch.cuda.current_stream().cuda_stream
@@ -242,7 +259,8 @@ def bench_batched(C, arith):
                         "log-uniform 1e3-1e6 turns (seed 20261203)",
             "particles": int(sum(s["n_particles"] for s in sets)),
             "nominal_particle_turns": nominal, "executed_particle_turns": float(steps_batch.sum()),
-            "batched_s": t_batch, "plain_sum_s": t_plain, "speedup": t_plain / t_batch,
+            "batched_s": t_batch, "one_group_s": t_one_group, "plain_sum_s": t_plain,
+            "speedup": t_plain / t_batch,
             "batched_value": nominal / t_batch, "survival_equal_to_plain": equal,
             "n_chunks": b.n_chunks(), "timing": "wall clock around synchronous runs, best of 2"}
 
@@ -307,13 +325,12 @@ def bench_adjoint(C):
             "timing": "CUDA events, best of 3 after one warm-up"}
 
 
-def bench_indicators(C, turns=100_000):
+def bench_indicators(C, turns=100_000, side=512):
     """Tangent map + indicators fused: 512x512 grid on [0, 0.4]^2, eps 32,
     mu 0, windows at the 13 log-spaced turns 1e2..1e5 (MEGNO, Birkhoff-MEGNO,
     Lyapunov with tangent vectors, Birkhoff tunes)."""
     import torch
 
-    side = 512
     v = np.linspace(0.0, 0.4, side)
     xx, yy = np.meshgrid(v, v)
     x, y = xx.ravel(), yy.ravel()
@@ -337,7 +354,7 @@ def bench_indicators(C, turns=100_000):
     run(1000)
     dt, p = run(turns)
     steps = p.get(C.FIELD_STEPS)
-    return {"workload": f"512x512 grid on [0,0.4]^2, eps 32, mu 0, {turns} turns, "
+    return {"workload": f"{side}x{side} grid on [0,0.4]^2, eps 32, mu 0, {turns} turns, "
                         "MEGNO + Birkhoff-MEGNO + Lyapunov + Birkhoff tunes at 13 windows",
             "seconds": dt, "nominal_particle_turns_per_s": n * turns / dt,
             "executed_particle_turns_per_s": float(steps.sum()) / dt,
@@ -345,6 +362,60 @@ def bench_indicators(C, turns=100_000):
 
 
 # ---- reference arm ---------------------------------------------------------------
+
+def bench_tunes(C, turns=10_000, side=128):
+    """all_tunes of a 128x128 grid on [0, 0.5]^2 (eps 16, mu 0.2): the orbit
+    of 1e4 turns is recorded on the device, its mean removed, then Birkhoff
+    and FFT tunes of the windows [0, 1000], [1000, 5000], [5000, 1e4] and of
+    the full orbit."""
+    import torch
+
+    v = np.linspace(0.0, 0.5, side)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    z = np.zeros_like(x)
+    n = x.size
+    frm, to = [0, turns // 10, turns // 2], [turns // 10, turns // 2, turns]
+
+    def run():
+        tr = C.Tracker(turns, 0.168, 0.201, "sps", float("nan"), 16.0, 0)
+        p = C.Particles(x, z, y, z)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b, f = C.tracker_orbit_tunes(tr, p, turns, 0.2, 10.0, frm, to, True, True)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, b
+
+    run()
+    dt, b = run()
+    orbit_bytes = 32.0 * n * (turns + 1)
+    return {"workload": f"{side}x{side} grid on [0,0.5]^2, eps 16, mu 0.2, {turns} turns, "
+                        "orbit recorded, mean removed, Birkhoff + FFT tunes of 3 windows "
+                        "and the full orbit",
+            "seconds": dt, "nominal_particle_turns_per_s": n * turns / dt,
+            "orbit_bytes": orbit_bytes, "orbit_gb_per_s": orbit_bytes / dt / 1e9,
+            "finite_tunes": int(np.isfinite(b).sum()),
+            "timing": "wall clock around one synchronous call (record + tunes)"}
+
+
+def run_only(args):
+    import torch
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    from henon_map_cpp_b200 import _capi as C
+
+    arith = C.ARITH_FAST if args.arith == "fast" else C.ARITH_EXACT
+    kw = {}
+    if args.extra_side is not None:
+        kw["side"] = args.extra_side
+    if args.extra_turns is not None:
+        kw["turns"] = args.extra_turns
+    fn = {"batched": lambda: bench_batched(C, arith), "adjoint": lambda: bench_adjoint(C),
+          "indicators": lambda: bench_indicators(C, **kw),
+          "tunes": lambda: bench_tunes(C, **kw)}[args.only]
+    print(json.dumps({"only": args.only, **fn()}), flush=True)
+
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -434,6 +505,8 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    work = {}
+
     def timed(mode, n_steps, n_warm):
         for _ in range(n_warm):
             one_step(mode)
@@ -453,6 +526,7 @@ def run_ours(args):
             executed += e
             flops += f
         kernel_ms, launches = C.get_profile()
+        work["list_particles"], work["chunk_turns"] = C.get_profile_work()
         C.set_profiling(False)
         barrier()
         return total_ms, executed, flops, kernel_ms, launches
@@ -460,6 +534,12 @@ def run_ours(args):
     with ClockSampler(local) as clocks:
         total_ms, executed, flops, kernel_ms, launches = timed(arith, args.steps, args.warmup)
     clock_summary = clocks.summary()
+    # Bytes per launch: algorithmic (36 B in + 36 B out per list particle,
+    # 32 B of records per turn) and DRAM traffic scaled from an ncu capture
+    # of the same kernel (NCU_BYTES_PER_LIST_PARTICLE).
+    lp, ct = work["list_particles"], work["chunk_turns"]
+    algo_bytes = (72.0 * lp + 32.0 * ct) / launches if launches else None
+    traffic = (NCU_BYTES_PER_LIST_PARTICLE * lp + 32.0 * ct) / launches if launches else None
 
     # Whole-job numbers: max time over ranks, sum of work.
     if dist is not None:
@@ -539,6 +619,7 @@ def run_ours(args):
         extras["batched"] = bench_batched(C, arith)
         extras["adjoint"] = bench_adjoint(C)
         extras["indicators"] = bench_indicators(C)
+        extras["tunes"] = bench_tunes(C)
 
     if rank == 0:
         peak_unit = "TFLOP/s"
@@ -552,7 +633,11 @@ def run_ours(args):
             "survivor_fraction": executed / nominal,
             "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tflops,
                          "unit": peak_unit, "frac": achieved_tf / peak_tflops if peak_tflops else None,
-                         "traffic": None,
+                         "traffic": traffic,
+                         "traffic_source": "bytes per launch: DRAM read+write per list particle "
+                                           "from ncu (32.1 B, 512^2 DA scan, staged kernel) x list "
+                                           "particles + 32 B of records per turn",
+                         "algorithmic_bytes": algo_bytes,
                          "peak_source": "FP64 FMA-chain microbenchmark in this process "
                                         "(hm_fp64_peak; FMA = 2 flops)",
                          "kernel": "track_chunk_kernel", "kernel_ms": kernel_ms,
@@ -577,6 +662,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.only:
+        run_only(args)
     else:
         run_ours(args)
 

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "hm_fp64_peak": (None, [c_double, _PD, _PD]),
     "hm_set_profiling": (None, [c_int]),
     "hm_get_profile": (None, [_PD, POINTER(c_uint64)]),
+    "hm_get_profile_work": (None, [c_void_p, c_void_p]),
     # tangent map
     "hm_matrices_create": (None, [c_size_t, POINTER(c_void_p)]),
     "hm_matrices_destroy": (None, [c_void_p]),
@@ -163,6 +164,7 @@ _SIGNATURES = {
     "hm_batch_create": (None, [c_size_t, c_void_p, POINTER(c_void_p)]),
     "hm_batch_destroy": (None, [c_void_p]),
     "hm_batch_configure": (None, [c_void_p, c_int, c_int, c_uint32, c_uint32]),
+    "hm_batch_set_groups": (None, [c_void_p, c_int]),
     "hm_batch_size": (None, [c_void_p, POINTER(c_uint64), POINTER(c_uint32)]),
     "hm_batch_load": (None, [c_void_p, _PD, _PD, _PD, _PD]),
     "hm_batch_run": (None, [c_void_p, c_int]),
@@ -621,10 +623,14 @@ class Batch(_Handle):
         call("hm_batch_create", len(sets), ctypes.cast(arr, c_void_p), ctypes.byref(self.h))
         self.n_total = sum(int(s["n_particles"]) for s in sets)
 
-    def configure(self, arith: int = ARITH_EXACT, per_thread: int = 2, chunk0: int = 512,
+    def configure(self, arith: int = ARITH_EXACT, per_thread: int = 1, chunk0: int = 512,
                   chunk_max: int = 16384):
         call("hm_batch_configure", self.h, int(arith), int(per_thread), int(chunk0),
              int(chunk_max))
+
+    def set_groups(self, groups: int) -> None:
+        """Number of concurrently tracked groups of sets (1..8)."""
+        call("hm_batch_set_groups", self.h, int(groups))
 
     def n_chunks(self) -> int:
         a, b = c_uint64(), c_uint32()
@@ -696,6 +702,13 @@ def get_track_staging() -> int:
     v = c_uint32()
     call("hm_get_track_staging", ctypes.byref(v))
     return int(v.value)
+
+
+def get_profile_work():
+    """(list particles, chunk turns) summed over the timed tracking launches."""
+    a, b = c_uint64(), c_uint64()
+    call("hm_get_profile_work", ctypes.byref(a), ctypes.byref(b))
+    return int(a.value), int(b.value)
 
 
 def set_profiling(on: bool) -> None:

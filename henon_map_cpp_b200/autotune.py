@@ -2,8 +2,9 @@
 
 Results never depend on the launch shape (the tests check this bit for bit),
 so the tuner only measures: it times candidate (threads per block,
-particles per thread, first chunk, chunk cap) shapes of the chunked
-tracker, and (particles per thread, chunk schedule) of the batched path, on
+particles per thread, first chunk, chunk cap, turn records per staged
+copy) shapes of the chunked tracker, and (groups, particles per thread,
+chunk schedule) of the batched path, on
 a calibration workload with CUDA events, and keeps the fastest.  Results
 are cached per GPU model and arithmetic in a JSON file next to this module
 (HENON_B200_TUNING overrides the path).
@@ -26,8 +27,20 @@ from . import _capi as C
 CACHE = Path(os.environ.get("HENON_B200_TUNING", Path(__file__).with_name("tuning.json")))
 
 TRACK_SPACE = {"threads": (64, 128, 256), "per_thread": (1, 2, 4), "chunk0": (256, 512, 1024),
-               "chunk_max": (8192, 16384, 32768)}
-BATCH_SPACE = {"per_thread": (1, 2, 4), "chunk0": (256, 512, 1024), "chunk_max": (8192, 16384)}
+               "chunk_max": (8192, 16384, 32768), "stage_turns": (0, 64, 256, 512)}
+
+
+def _set_shape(shape) -> None:
+    C.set_track_config(shape["threads"], shape["per_thread"], shape["chunk0"], shape["chunk_max"])
+    C.set_track_staging(shape.get("stage_turns", C.get_track_staging()))
+
+
+def _current_shape() -> dict:
+    shape = dict(zip(("threads", "per_thread", "chunk0", "chunk_max"), C.get_track_config()))
+    shape["stage_turns"] = C.get_track_staging()
+    return shape
+BATCH_SPACE = {"groups": (4, 1, 2, 8), "per_thread": (1, 2, 4), "chunk0": (256, 512, 1024),
+               "chunk_max": (8192, 16384)}
 
 
 def _device_name() -> str:
@@ -48,7 +61,7 @@ def time_track_shape(shape, arith: int, data, repeats: int = 2) -> float:
     import torch
 
     x, px, y, py, turns = data
-    C.set_track_config(shape["threads"], shape["per_thread"], shape["chunk0"], shape["chunk_max"])
+    _set_shape(shape)
     tr = C.Tracker(turns, 0.168, 0.201, "sps", float("nan"), 16.0, 0)
     tr.arith = arith
     n = x.size
@@ -76,7 +89,7 @@ def tune_track(arith: int = C.ARITH_EXACT, budget_s: float = 30.0, data=None):
     """Coordinate search over TRACK_SPACE from the default shape; returns
     (best shape, its time in ms, every timing)."""
     data = data or _calibration()
-    cur = dict(zip(("threads", "per_thread", "chunk0", "chunk_max"), C.get_track_config()))
+    cur = _current_shape()
     timings = {}
 
     def cost(shape):
@@ -98,7 +111,7 @@ def tune_track(arith: int = C.ARITH_EXACT, budget_s: float = 30.0, data=None):
                 c = cost(cand)
                 if c < best * 0.995:
                     best, cur, improved = c, cand, True
-    C.set_track_config(cur["threads"], cur["per_thread"], cur["chunk0"], cur["chunk_max"])
+    _set_shape(cur)
     return cur, best, {str(k): v for k, v in timings.items()}
 
 
@@ -108,14 +121,18 @@ def tune_batch(sets, coords, arith: int = C.ARITH_EXACT, budget_s: float = 30.0)
     b.load(*coords)
     res = {}
     start = time.perf_counter()
-    for k, c0, cm in itertools.product(*BATCH_SPACE.values()):
+    groups = None
+    for g, k, c0, cm in itertools.product(*BATCH_SPACE.values()):
         if cm < c0 or time.perf_counter() - start > budget_s:
             continue
+        if g != groups:
+            b.set_groups(g)
+            groups = g
         b.configure(arith, k, c0, cm)
         b.run(True)
         t0 = time.perf_counter()
         b.run(True)
-        res[(k, c0, cm)] = time.perf_counter() - t0
+        res[(g, k, c0, cm)] = time.perf_counter() - t0
     best = min(res, key=res.get)
     return dict(zip(BATCH_SPACE, best)), res[best], {str(k): v for k, v in res.items()}
 
@@ -140,5 +157,5 @@ def apply(arith: int = C.ARITH_EXACT, retune: bool = False, budget_s: float = 30
         except OSError:
             pass
     shape = cache[key]["track"]
-    C.set_track_config(shape["threads"], shape["per_thread"], shape["chunk0"], shape["chunk_max"])
+    _set_shape(shape)
     return shape

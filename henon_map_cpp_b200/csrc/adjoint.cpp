@@ -42,11 +42,22 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, c
         return fail(HM_ERR_INVALID_ARG, "the adjoint needs checkpoint_every > 0, a workspace and "
                                         "gradient outputs");
     if (mode == 1 && !grad_ic) return fail(HM_ERR_INVALID_ARG, "null gradient output");
-    std::vector<double> ripple;
-    if (reverse) HM_TRY(hm::modulation_ripple(t->kind, n_turns, t->omega_0, t->offset, ripple));
-    DeviceBuffer dS, dw;
-    HM_TRY(hm::upload(dS, ripple));
-    HM_TRY(hm::upload(dw, hm::birkhoff_weights(n_turns)));
+    std::lock_guard<std::mutex> lock(t->adjoint_mutex);
+    if (!t->adjoint_cached || t->adjoint_turns != n_turns) {
+        HM_TRY(hm::upload(t->adjoint_w, hm::birkhoff_weights(n_turns)));
+        t->adjoint_S.release();
+        t->adjoint_turns = n_turns;
+        t->adjoint_cached = true;
+        t->adjoint_has_ripple = false;
+    }
+    if (reverse && !t->adjoint_has_ripple) {
+        // Only the reverse sweeps need d omega / d theta (and an "sps" or
+        // "basic" modulation).
+        std::vector<double> ripple;
+        HM_TRY(hm::modulation_ripple(t->kind, n_turns, t->omega_0, t->offset, ripple));
+        HM_TRY(hm::upload(t->adjoint_S, ripple));
+        t->adjoint_has_ripple = true;
+    }
     hm::AdjointArgs a{};
     a.x0 = x0;
     a.px0 = px0;
@@ -54,8 +65,8 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, c
     a.py0 = py0;
     a.n = n;
     a.table = t->table.as<double>();
-    a.S = dS.as<double>();
-    a.w = dw.as<double>();
+    a.S = t->adjoint_S.as<double>();
+    a.w = t->adjoint_w.as<double>();
     a.n_turns = n_turns;
     a.ckpt = checkpoint_every ? checkpoint_every : 1;
     a.mu = mu;

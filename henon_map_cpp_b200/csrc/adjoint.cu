@@ -39,6 +39,40 @@ struct S4 {
     double x, px, y, py;
 };
 
+// The inverse-sweep kernel walks the turns in step across its block, so it
+// stages each turn's records -- the rotation record, w_k and S_k -- through
+// shared memory: while the block runs the kStage turns of one stage, each
+// thread holds kPerThread doubles of the next stage in registers (plain
+// loads, issued a whole stage ahead of use) and stores them into the other
+// buffer at the end of the stage.  The launch often holds few warps per
+// SM, too few to hide per-turn L2 latency otherwise.
+constexpr int kThreads = 128;
+constexpr uint32_t kStage = 64u;
+constexpr int kRec = 6;  // doubles per turn: sin wx, cos wx, sin wy, cos wy, w_k, S_k
+constexpr int kPerThread = int(kStage) * kRec / kThreads;
+static_assert(kPerThread * kThreads == int(kStage) * kRec, "stage must split evenly");
+
+// Records of turns [lo, lo + kn) into registers, element e = 6 (turn - lo) + field.
+__device__ __forceinline__ void rec_load(double (&r)[kPerThread], const AdjointArgs &a,
+                                         uint32_t lo, uint32_t kn) {
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {
+        const uint32_t e = threadIdx.x + uint32_t(kThreads * q);
+        const uint32_t t = e / uint32_t(kRec), f = e % uint32_t(kRec);
+        double v = 0.0;
+        if (t < kn) {
+            const size_t k = size_t(lo) + t;
+            v = f < 4u ? a.table[4u * k + f] : (f == 4u ? a.w[k] : a.S[k]);
+        }
+        r[q] = v;
+    }
+}
+
+__device__ __forceinline__ void rec_store(double *buf, const double (&r)[kPerThread]) {
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) buf[threadIdx.x + uint32_t(kThreads * q)] = r[q];
+}
+
 // One forward turn; returns x^2+px^2+y^2+py^2 of the new state in the
 // tracker's grouping (the loss uses the same number).
 template <int ARITH, bool OCT>
@@ -160,87 +194,139 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const AdjointArgs a) {
 // errors of the reconstruction can grow only across one segment, and the
 // per-turn memory traffic of the replay variant disappears.
 template <int ARITH, bool OCT>
-__global__ void __launch_bounds__(128) adjoint_inverse_kernel(const AdjointArgs a) {
+__global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const AdjointArgs a) {
+    __shared__ __align__(16) double recs[2][kStage * kRec];
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+    const bool in_range = i < a.n;
+    const size_t ii = in_range ? i : 0;
     const size_t n = a.n;
     const uint32_t N = a.n_turns, C = a.ckpt;
-    S4 s{a.x0[i], a.px0[i], a.y0[i], a.py0[i]};
-    bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
-    double loss = 0.0;
-    uint32_t k = 0;
-    for (; alive && k < N; ++k) {
-        if (k % C == 0) store4(a.ckpt_buf, k / C, n, i, s);
-        const double r = fwd<ARITH, OCT>(s, dev::load_turn(a.table, k), a.mu);
-        if (!inside(r, a.b2bits)) {
-            alive = false;
-            break;
-        }
-        loss = fma(a.w[k], r, loss);
-    }
-    a.steps[i] = alive ? N : k;
-    if (!alive) {
-        a.loss[i] = 0.0;
-        a.survived[i] = 0;
-        a.g_ic[i] = a.g_ic[n + i] = a.g_ic[2 * n + i] = a.g_ic[3 * n + i] = 0.0;
-        a.g_th[i] = a.g_th[n + i] = a.g_th[2 * n + i] = a.g_th[3 * n + i] = 0.0;
-        return;
-    }
-    a.loss[i] = loss;
-    a.survived[i] = 1;
+    const uint32_t n_stages = (N + kStage - 1) / kStage;
+    S4 s{a.x0[ii], a.px0[ii], a.y0[ii], a.py0[ii]};
+    bool alive = in_range && !dev::is_lost(s.x, s.px, s.y, s.py);
+    double next[kPerThread];
 
+    // ---- forward sweep: loss and checkpoints ----------------------------------
+    double loss = 0.0;
+    uint32_t lost_at = N;
+    uint32_t next_ckpt = 0;  // turn of the next checkpoint store
+    if (n_stages > 0) {
+        rec_load(next, a, 0u, min(kStage, N));
+        rec_store(recs[0], next);
+    }
+    __syncthreads();
+    for (uint32_t sg = 0; sg < n_stages; ++sg) {
+        const uint32_t k0 = sg * kStage, kn = min(kStage, N - k0);
+        const bool more = sg + 1 < n_stages;
+        if (more) rec_load(next, a, k0 + kStage, min(kStage, N - k0 - kStage));
+        const double *R = recs[sg & 1u];
+        for (uint32_t kk = 0; alive && kk < kn; ++kk) {
+            const uint32_t k = k0 + kk;
+            if (k == next_ckpt) {
+                store4(a.ckpt_buf, k / C, n, i, s);
+                next_ckpt += C;
+            }
+            const double *rr = R + kRec * kk;
+            const double r = fwd<ARITH, OCT>(s, dev::Turn{rr[0], rr[1], rr[2], rr[3]}, a.mu);
+            if (!inside(r, a.b2bits)) {
+                alive = false;
+                lost_at = k;
+                break;
+            }
+            loss = fma(rr[4], r, loss);
+        }
+        // The other buffer was last read in the previous stage, which the
+        // whole block has finished; the barrier publishes the stores.
+        if (more) rec_store(recs[(sg + 1u) & 1u], next);
+        if (!__syncthreads_or(alive)) break;
+    }
+    if (in_range) {
+        a.steps[i] = alive ? N : lost_at;
+        a.loss[i] = alive ? loss : 0.0;
+        a.survived[i] = alive ? 1 : 0;
+    }
+
+    // ---- reverse sweep: turns N-1 .. 0 --------------------------------------------
     const double mu = a.mu;
     double lx = 0.0, lpx = 0.0, ly = 0.0, lpy = 0.0;
     // sum_k gw_k and sum_k S_k gw_k per plane: the parameter gradients are
     // combined from them at the end.
     double Gx = 0.0, Gy = 0.0, Hx = 0.0, Hy = 0.0, g_mu = 0.0;
-    const S4 final_state = s;
+    S4 post = s;  // the state after turn N-1
     const uint32_t n_seg = (N + C - 1) / C;
-    for (int seg = int(n_seg) - 1; seg >= 0; --seg) {
-        const uint32_t k0 = uint32_t(seg) * C;
-        const uint32_t k1 = min(k0 + C, N);
-        S4 post = (uint32_t(seg) + 1 < n_seg) ? load4(a.ckpt_buf, uint32_t(seg) + 1, n, i) : final_state;
-        for (uint32_t kk = k1; kk-- > k0;) {
-            const dev::Turn t = dev::load_turn(a.table, kk);
-            const double X = post.x, PX = post.px, Y = post.y, PY = post.py;
-            // inverse turn (henon_step reverse order, src/henon.cu:510-528)
-            const double x = fma(t.cx, X, -t.sx * PX), px1 = fma(t.sx, X, t.cx * PX);
-            const double y = fma(t.cy, Y, -t.sy * PY), py1 = fma(t.sy, Y, t.cy * PY);
-            const double xx = x * x, yy = y * y;
-            const double dxy = xx - yy;
-            const double ax3 = fma(-3.0, yy, xx), ay3 = fma(-3.0, xx, yy);
-            double qx = dxy, qy = -2.0 * x * y;
-            if (OCT) {
-                qx = fma(mu * x, ax3, qx);
-                qy = fma(mu * y, ay3, qy);
+    // Turns left in the current segment; at 0 the next (earlier) segment
+    // starts from its stored end state, the checkpoint after it.
+    uint32_t seg_left = N - (n_seg ? n_seg - 1u : 0u) * C;
+    if (__syncthreads_or(alive) && n_stages > 0) {
+        rec_load(next, a, N - min(kStage, N), min(kStage, N));
+        rec_store(recs[0], next);
+        __syncthreads();
+        for (uint32_t sg = 0; sg < n_stages; ++sg) {
+            const uint32_t k0 = sg * kStage, kn = min(kStage, N - k0);
+            const bool more = sg + 1 < n_stages;
+            if (more) {
+                const uint32_t kn2 = min(kStage, N - k0 - kStage);
+                rec_load(next, a, N - k0 - kStage - kn2, kn2);
             }
-            post = S4{x, px1 - qx, y, py1 - qy};
-            // adjoint of the post-turn state: lambda + w_k grad A
-            const double w2 = 2.0 * a.w[kk];
-            const double aX = fma(w2, X, lx), aPX = fma(w2, PX, lpx);
-            const double aY = fma(w2, Y, ly), aPY = fma(w2, PY, lpy);
-            const double gwx = fma(aX, PX, -aPX * X);
-            const double gwy = fma(aY, PY, -aPY * Y);
-            const double Sk = a.S[kk];
-            Gx += gwx;
-            Gy += gwy;
-            Hx = fma(Sk, gwx, Hx);
-            Hy = fma(Sk, gwy, Hy);
-            const double rx = fma(t.cx, aX, -t.sx * aPX), rpx = fma(t.sx, aX, t.cx * aPX);
-            const double ry = fma(t.cy, aY, -t.sy * aPY), rpy = fma(t.sy, aY, t.cy * aPY);
-            double da = 2.0 * x, db = -2.0 * y, dd = -2.0 * x;
-            if (OCT) {
-                da = fma(3.0 * mu, dxy, da);
-                db = fma(-6.0 * mu * x, y, db);
-                dd = fma(-3.0 * mu, dxy, dd);
+            // records of the table span [N - k0 - kn, N - k0), ascending
+            const double *R = recs[sg & 1u];
+            for (uint32_t j = 0; alive && j < kn; ++j) {
+                const uint32_t kk = N - 1u - (k0 + j);  // turn index, descending
+                if (seg_left == 0u) {
+                    post = load4(a.ckpt_buf, (kk + 1u) / C, n, i);
+                    seg_left = C;
+                }
+                --seg_left;
+                const double *rr = R + kRec * (kn - 1u - j);
+                const dev::Turn t{rr[0], rr[1], rr[2], rr[3]};
+                const double X = post.x, PX = post.px, Y = post.y, PY = post.py;
+                // inverse turn (henon_step reverse order, src/henon.cu:510-528)
+                const double x = fma(t.cx, X, -t.sx * PX), px1 = fma(t.sx, X, t.cx * PX);
+                const double y = fma(t.cy, Y, -t.sy * PY), py1 = fma(t.sy, Y, t.cy * PY);
+                const double xx = x * x, yy = y * y;
+                const double dxy = xx - yy;
+                const double ax3 = fma(-3.0, yy, xx), ay3 = fma(-3.0, xx, yy);
+                double qx = dxy, qy = -2.0 * x * y;
+                if (OCT) {
+                    qx = fma(mu * x, ax3, qx);
+                    qy = fma(mu * y, ay3, qy);
+                }
+                post = S4{x, px1 - qx, y, py1 - qy};
+                // adjoint of the post-turn state: lambda + w_k grad A
+                const double w2 = 2.0 * rr[4];
+                const double aX = fma(w2, X, lx), aPX = fma(w2, PX, lpx);
+                const double aY = fma(w2, Y, ly), aPY = fma(w2, PY, lpy);
+                const double gwx = fma(aX, PX, -aPX * X);
+                const double gwy = fma(aY, PY, -aPY * Y);
+                const double Sk = rr[5];
+                Gx += gwx;
+                Gy += gwy;
+                Hx = fma(Sk, gwx, Hx);
+                Hy = fma(Sk, gwy, Hy);
+                const double rx = fma(t.cx, aX, -t.sx * aPX), rpx = fma(t.sx, aX, t.cx * aPX);
+                const double ry = fma(t.cy, aY, -t.sy * aPY), rpy = fma(t.sy, aY, t.cy * aPY);
+                double da = 2.0 * x, db = -2.0 * y, dd = -2.0 * x;
+                if (OCT) {
+                    da = fma(3.0 * mu, dxy, da);
+                    db = fma(-6.0 * mu * x, y, db);
+                    dd = fma(-3.0 * mu, dxy, dd);
+                }
+                // d(px1, py1)/d mu = (x (x^2 - 3y^2), y (y^2 - 3x^2)), also at mu = 0
+                g_mu = fma(rpx, x * ax3, fma(rpy, y * ay3, g_mu));
+                lx = fma(rpx, da, fma(rpy, db, rx));
+                ly = fma(rpx, db, fma(rpy, dd, ry));
+                lpx = rpx;
+                lpy = rpy;
             }
-            // d(px1, py1)/d mu = (x (x^2 - 3y^2), y (y^2 - 3x^2)), also at mu = 0
-            g_mu = fma(rpx, x * ax3, fma(rpy, y * ay3, g_mu));
-            lx = fma(rpx, da, fma(rpy, db, rx));
-            ly = fma(rpx, db, fma(rpy, dd, ry));
-            lpx = rpx;
-            lpy = rpy;
+            if (more) rec_store(recs[(sg + 1u) & 1u], next);
+            __syncthreads();
         }
+    }
+    if (!in_range) return;
+    if (!alive) {
+        a.g_ic[i] = a.g_ic[n + i] = a.g_ic[2 * n + i] = a.g_ic[3 * n + i] = 0.0;
+        a.g_th[i] = a.g_th[n + i] = a.g_th[2 * n + i] = a.g_th[3 * n + i] = 0.0;
+        return;
     }
     a.g_ic[i] = lx;
     a.g_ic[n + i] = lpx;
@@ -314,8 +400,8 @@ cudaError_t launch_a(const AdjointArgs &a, int mode, cudaStream_t s) {
         if (oct) adjoint_kernel<ARITH, true><<<blocks, 128, 0, s>>>(a);
         else adjoint_kernel<ARITH, false><<<blocks, 128, 0, s>>>(a);
     } else if (mode == 3) {
-        if (oct) adjoint_inverse_kernel<ARITH, true><<<blocks, 128, 0, s>>>(a);
-        else adjoint_inverse_kernel<ARITH, false><<<blocks, 128, 0, s>>>(a);
+        if (oct) adjoint_inverse_kernel<ARITH, true><<<blocks, kThreads, 0, s>>>(a);
+        else adjoint_inverse_kernel<ARITH, false><<<blocks, kThreads, 0, s>>>(a);
     } else if (mode == 1) {
         if (oct) forward_loss_kernel<ARITH, true, true><<<blocks, 128, 0, s>>>(a);
         else forward_loss_kernel<ARITH, false, true><<<blocks, 128, 0, s>>>(a);

@@ -10,8 +10,10 @@
 //     at once and appends survivors to its set's next list;
 //   * batch_plan_kernel -- one block: per-set survivor counts -> next tile
 //     table (prefix sum), counters reset, ping-pong parity flipped.
-// The whole sequence (init, plan, n_chunks x (chunk, plan)) has a fixed
-// shape, so the host captures it once in a CUDA graph and replays it.
+// The sets are split into groups, each with its own chain of (plan, chunk)
+// launches and its own tile table and counters; the chains run on separate
+// streams.  The whole sequence has a fixed shape, so the host captures it
+// once in a CUDA graph and replays it.
 //
 // The per-particle arithmetic is the tracking kernel's (track.cu), so every
 // set's result is bit-identical to a plain hm_track of that set.
@@ -27,11 +29,38 @@ namespace {
 
 using dev::Particle;
 
+// Each warp of the persistent chunk kernel works on tiles of different
+// sets, so every warp stages its own set's turn records through shared
+// memory: while the warp runs the kStageTurns turns of one stage, each lane
+// holds kPerLane doubles of the next stage in registers (one coalesced
+// 256-byte load per kPerLane), and stores them into the warp's other buffer
+// at the end of the stage.  Without it, a warp whose set has few particles
+// left waits on an L2 round trip every few turns.
+constexpr uint32_t kStageTurns = 32u;
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+constexpr int kPerLane = int(kStageTurns) * 4 / 32;
+
+// Records [lo, lo + kn) of a table; element e of the stage = table[4 lo + e].
+__device__ __forceinline__ void stage_load(double (&r)[kPerLane], const double *table, uint32_t lo,
+                                           uint32_t kn, unsigned lane) {
+#pragma unroll
+    for (int q = 0; q < kPerLane; ++q) {
+        const uint32_t e = lane + 32u * uint32_t(q);
+        r[q] = e < 4u * kn ? __ldg(table + 4u * size_t(lo) + e) : 0.0;
+    }
+}
+
+__device__ __forceinline__ void stage_store(double *buf, const double (&r)[kPerLane],
+                                            unsigned lane) {
+#pragma unroll
+    for (int q = 0; q < kPerLane; ++q) buf[lane + 32u * uint32_t(q)] = r[q];
+}
+
 // Copies every non-NaN particle of every set into list 0 of its set and
 // counts them (check_nan: NaN particles are never touched).
 __global__ void batch_init_kernel(BatchDev b) {
     const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i == 0) *b.parity = 1u;  // the first plan flips it to list 0
     if (i >= b.n_total) return;
     const uint32_t s = b.particle_set[i];
     const double x = b.x[i], px = b.px[i], y = b.y[i], py = b.py[i];
@@ -70,7 +99,9 @@ __global__ void batch_plan_kernel(BatchDev b, uint32_t chunk_len_done, uint32_t 
         }
         *b.n_tiles = total;
         *b.next_item = 0u;
-        *b.parity ^= 1u;
+        // The first plan of a chain reads list 0, where the collection put
+        // every particle; each later one swaps the lists.
+        *b.parity = chunk_len_done == 0u ? 0u : (*b.parity ^ 1u);
     }
     __syncthreads();
     if (s < b.n_sets) {
@@ -82,7 +113,7 @@ __global__ void batch_plan_kernel(BatchDev b, uint32_t chunk_len_done, uint32_t 
 template <int ARITH, bool OCT, int K>
 __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &set,
                                          const BatchStateDev &st, uint32_t s, uint32_t start,
-                                         int in, int out) {
+                                         int in, int out, double *bufs) {
     const unsigned lane = threadIdx.x & 31u;
     Particle p[K];
     uint64_t id[K];
@@ -102,33 +133,53 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
     const double mu = set.mu;
     const dev::Barrier bar = dev::make_barrier<ARITH>(set.b2bits);
     bool warp_live = __any_sync(dev::kFullMask, any);
-    dev::Turn t = nt ? dev::load_turn(set.table, turn0) : dev::Turn{0.0, 0.0, 0.0, 0.0};
-    for (uint32_t k = 0; warp_live && k < nt; ++k) {
-        const uint32_t kn = (k + 1 < nt) ? k + 1 : k;
-        const dev::Turn tn = dev::load_turn(set.table, turn0 + kn);
-        bool any_check = false;
-        bool check[K];
-        double r[K];
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            r[j] = dev::turn<ARITH, OCT, false>(p[j], t, mu);
-            check[j] = live[j] && !dev::surely_inside(r[j], bar);
-            any_check |= check[j];
-        }
-        if (__any_sync(dev::kFullMask, any_check)) {
-            bool still = false;
+    const uint32_t n_stages = (nt + kStageTurns - 1) / kStageTurns;
+    double next[kPerLane];
+    if (warp_live && n_stages > 0) {
+        stage_load(next, set.table, turn0, min(kStageTurns, nt), lane);
+        stage_store(bufs, next, lane);
+    }
+    __syncwarp();
+    for (uint32_t sg = 0; warp_live && sg < n_stages; ++sg) {
+        const uint32_t k0 = sg * kStageTurns, kn_stage = min(kStageTurns, nt - k0);
+        const bool more = sg + 1 < n_stages;
+        if (more)
+            stage_load(next, set.table, turn0 + k0 + kStageTurns,
+                       min(kStageTurns, nt - k0 - kStageTurns), lane);
+        const double *rec = bufs + (sg & 1u) * kStageTurns * 4u;
+#pragma unroll 2
+        for (uint32_t kk = 0; warp_live && kk < kn_stage; ++kk) {
+            const uint32_t k = k0 + kk;
+            const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * kk);
+            const double2 q0 = q[0], q1 = q[1];
+            const dev::Turn t{q0.x, q0.y, q1.x, q1.y};
+            bool any_check = false;
+            bool check[K];
+            double r[K];
 #pragma unroll
             for (int j = 0; j < K; ++j) {
-                if (check[j] && !dev::settle_inside<ARITH>(r[j], p[j], bar)) {
-                    b.x[id[j]] = b.px[id[j]] = b.y[id[j]] = b.py[id[j]] = dev::quiet_nan();
-                    b.steps[id[j]] = turn0 + k;
-                    live[j] = false;
-                }
-                still |= live[j];
+                r[j] = dev::turn<ARITH, OCT, false>(p[j], t, mu);
+                check[j] = live[j] && !dev::surely_inside(r[j], bar);
+                any_check |= check[j];
             }
-            warp_live = __any_sync(dev::kFullMask, still);
+            if (__any_sync(dev::kFullMask, any_check)) {
+                bool still = false;
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    if (check[j] && !dev::settle_inside<ARITH>(r[j], p[j], bar)) {
+                        b.x[id[j]] = b.px[id[j]] = b.y[id[j]] = b.py[id[j]] = dev::quiet_nan();
+                        b.steps[id[j]] = turn0 + k;
+                        live[j] = false;
+                    }
+                    still |= live[j];
+                }
+                warp_live = __any_sync(dev::kFullMask, still);
+            }
         }
-        t = tn;
+        // The other buffer was last read in the previous stage, which every
+        // lane has finished.
+        if (more) stage_store(bufs + ((sg + 1u) & 1u) * kStageTurns * 4u, next, lane);
+        __syncwarp();
     }
     const bool final_chunk = turn0 + nt == set.n_turns;
 #pragma unroll
@@ -162,8 +213,10 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
 
 // Persistent: warps pop warp-tiles until the chunk's queue is empty.
 template <int ARITH, int K>
-__global__ void __launch_bounds__(128) batch_chunk_kernel(BatchDev b) {
+__global__ void __launch_bounds__(kThreads) batch_chunk_kernel(BatchDev b) {
+    __shared__ __align__(16) double stage_bufs[kWarps][2 * kStageTurns * 4];
     const unsigned lane = threadIdx.x & 31u;
+    double *bufs = stage_bufs[threadIdx.x >> 5];
     const uint32_t n_tiles = *b.n_tiles;
     const int in = int(*b.parity), out = 1 - in;
     while (true) {
@@ -176,9 +229,9 @@ __global__ void __launch_bounds__(128) batch_chunk_kernel(BatchDev b) {
         const BatchSetDev &set = b.sets[s];
         const uint32_t start = (item - st.first_tile) * 32u * uint32_t(K);
         if (set.mu != 0.0)
-            run_tile<ARITH, true, K>(b, set, st, s, start, in, out);
+            run_tile<ARITH, true, K>(b, set, st, s, start, in, out, bufs);
         else
-            run_tile<ARITH, false, K>(b, set, st, s, start, in, out);
+            run_tile<ARITH, false, K>(b, set, st, s, start, in, out, bufs);
     }
 }
 
@@ -198,7 +251,7 @@ cudaError_t launch_batch_plan(const BatchDev &b, uint32_t done_len, uint32_t nex
 
 cudaError_t launch_batch_chunk(const BatchDev &b, int blocks, cudaStream_t s) {
     const int a = b.arith, k = b.per_thread;
-#define HM_BATCH_LAUNCH(A, KK) batch_chunk_kernel<A, KK><<<blocks, 128, 0, s>>>(b)
+#define HM_BATCH_LAUNCH(A, KK) batch_chunk_kernel<A, KK><<<blocks, kThreads, 0, s>>>(b)
     if (a == HM_ARITH_FAST) {
         if (k == 1) HM_BATCH_LAUNCH(HM_ARITH_FAST, 1);
         else if (k == 2) HM_BATCH_LAUNCH(HM_ARITH_FAST, 2);
@@ -216,13 +269,13 @@ int batch_chunk_blocks_per_sm(int arith, int per_thread) {
     int n = 0;
     cudaError_t e;
     if (arith == HM_ARITH_FAST)
-        e = per_thread == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 1>, 128, 0)
-            : per_thread == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 2>, 128, 0)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 4>, 128, 0);
+        e = per_thread == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 1>, kThreads, 0)
+            : per_thread == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 2>, kThreads, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_FAST, 4>, kThreads, 0);
     else
-        e = per_thread == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 1>, 128, 0)
-            : per_thread == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 2>, 128, 0)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 4>, 128, 0);
+        e = per_thread == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 1>, kThreads, 0)
+            : per_thread == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 2>, kThreads, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_chunk_kernel<HM_ARITH_EXACT, 4>, kThreads, 0);
     return e == cudaSuccess && n > 0 ? n : 1;
 }
 

@@ -45,6 +45,8 @@ struct Profile {
     std::mutex mutex;
     double kernel_ms = 0.0;
     uint64_t launches = 0;
+    uint64_t list_particles = 0;  // particles of the input lists, summed over launches
+    uint64_t chunk_turns = 0;     // turns of the launches, summed
 };
 Profile g_profile;
 
@@ -69,6 +71,7 @@ struct LaunchTimer {
     void end(cudaStream_t s) {
         if (armed) cudaEventRecord(stop, s);
     }
+    uint64_t particles = 0, turns = 0;  // work of the armed launch
     void collect() {  // call after the stream has been synchronised
         if (!armed) return;
         float ms = 0.f;
@@ -76,6 +79,8 @@ struct LaunchTimer {
             std::lock_guard<std::mutex> lock(g_profile.mutex);
             g_profile.kernel_ms += ms;
             g_profile.launches += 1;
+            g_profile.list_particles += particles;
+            g_profile.chunk_turns += turns;
         }
         armed = false;
     }
@@ -266,6 +271,8 @@ hm_status track_driver(double *x, double *px, double *y, double *py,
         timer.begin(stream);
         HM_CUDA_TRY(launch_track_chunk(c, l, n_in, stream));
         timer.end(stream);
+        timer.particles = n_in;
+        timer.turns = len;
         done += len;
         chunk = std::min<uint32_t>(chunk * 2u, cfg.chunk_max);
         if (last) break;
@@ -316,6 +323,15 @@ hm_status set_profiling(int on) {
     g_profile.enabled.store(on != 0);
     g_profile.kernel_ms = 0.0;
     g_profile.launches = 0;
+    g_profile.list_particles = 0;
+    g_profile.chunk_turns = 0;
+    return ok();
+}
+
+hm_status get_profile_work(uint64_t *list_particles, uint64_t *chunk_turns) {
+    std::lock_guard<std::mutex> lock(g_profile.mutex);
+    if (list_particles) *list_particles = g_profile.list_particles;
+    if (chunk_turns) *chunk_turns = g_profile.chunk_turns;
     return ok();
 }
 
@@ -400,6 +416,11 @@ hm_status compute_tables(hm_tracker *t, uint32_t n_turns, double omega_x, double
     std::vector<double> wx, wy;
     HM_TRY(hm::modulation(kind, n_turns, omega_x, omega_y, omega_0, epsilon, offset, wx, wy));
     HM_TRY(upload_tables(t, wx, wy));
+    {
+        // the adjoint's ripple follows the modulation
+        std::lock_guard<std::mutex> lock(t->adjoint_mutex);
+        t->adjoint_cached = false;
+    }
     t->kind = kind;
     t->omega_x = omega_x;
     t->omega_y = omega_y;
@@ -486,6 +507,10 @@ hm_status hm_set_profiling(int on) { return hm::set_profiling(on); }
 
 hm_status hm_get_profile(double *kernel_ms, uint64_t *launches) {
     return hm::get_profile(kernel_ms, launches);
+}
+
+hm_status hm_get_profile_work(uint64_t *list_particles, uint64_t *chunk_turns) {
+    return hm::get_profile_work(list_particles, chunk_turns);
 }
 
 // ---- host numerics ----------------------------------------------------------------

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -105,6 +106,13 @@ struct hm_tracker {
     std::string kind = "sps";
     double omega_x = 0.0, omega_y = 0.0, omega_0 = 0.0, epsilon = 0.0;
     uint32_t offset = 0;
+    // Birkhoff weights and modulation ripple of the last hm_adjoint turn
+    // count, kept on the device between calls (rebuilt when the turn count
+    // or the tables change); the mutex serialises adjoint calls.
+    mutable std::mutex adjoint_mutex;
+    mutable hm::DeviceBuffer adjoint_w, adjoint_S;
+    mutable uint32_t adjoint_turns = 0;
+    mutable bool adjoint_cached = false, adjoint_has_ripple = false;
 };
 
 namespace hm {

@@ -59,7 +59,7 @@ def sweep_sets(omega_pairs, epsilons, mus, n_particles: int, n_turns: int,
             for (wx, wy) in omega_pairs for e in epsilons for m in mus]
 
 
-def run_sweep(sets, coords, arith: int = C.ARITH_EXACT, per_thread: int = 2,
+def run_sweep(sets, coords, arith: int = C.ARITH_EXACT, per_thread: int = 1,
               chunk0: int = 512, chunk_max: int = 16384, use_graph: bool = True):
     """Tracks every set to its budget in one batch; returns a list with one
     dict per set: x, px, y, py (final) and steps (survival turns)."""

@@ -410,6 +410,11 @@ hm_status hm_batch_destroy(hm_batch *b);
  * chunk, cap of the doubling length); chosen by the autotuner. */
 hm_status hm_batch_configure(hm_batch *b, hm_arith arith, int per_thread,
                              uint32_t chunk0, uint32_t chunk_max);
+/* Splits the sets into `groups` (1..8) groups of about equal work, each
+ * tracked by its own chain of chunk launches on its own stream, so that
+ * one group's chunk ramp-down overlaps another group's work (default 4).
+ * Results do not depend on it. */
+hm_status hm_batch_set_groups(hm_batch *b, int groups);
 hm_status hm_batch_size(const hm_batch *b, uint64_t *n_total,
                         uint32_t *n_chunks);
 /* Initial conditions of all sets, concatenated in set order (host). */
@@ -517,6 +522,11 @@ hm_status hm_track_device_noalloc(double *x, double *px, double *y, double *py,
 hm_status hm_set_profiling(int on);
 /* Summed device time (ms) and number of timed tracking launches. */
 hm_status hm_get_profile(double *kernel_ms, uint64_t *launches);
+/* Work of the same timed launches: particles of their input lists and
+ * their turns, each summed over the launches (the units of the roofline's
+ * algorithmic bytes: 36 B in + 36 B out per list particle, 32 B of turn
+ * records per turn). */
+hm_status hm_get_profile_work(uint64_t *list_particles, uint64_t *chunk_turns);
 
 /* FP64 FMA-chain microbenchmark on the current device: *tflops receives
  * the achieved FP64 rate (an FMA counts as 2 flops). */

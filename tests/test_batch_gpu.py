@@ -93,3 +93,29 @@ def test_batch_barriers_at_the_last_bit(gpu, arith):
         if arith == 0:
             o = O.track(x, px, y, py, np.zeros(x.size, np.uint32), tabs, n_turns, mu, s["barrier"])
             np.testing.assert_array_equal(r["steps"], o[4])
+
+
+def test_batch_groups_do_not_change_results(gpu):
+    # Sets split into 1..8 concurrently tracked groups: each set still ends
+    # exactly as a plain hm_track of it alone.
+    sets, coords = sweep.heterogeneous_sets(seed=23, n_sets=11, n_range=(40, 2000),
+                                            turn_range=(50, 5000))
+    b = C.Batch(sets)
+    b.load(*coords)
+    outs = []
+    for g in (1, 3, 8):
+        b.set_groups(g)
+        b.configure(C.ARITH_EXACT, 1, 128, 1024)
+        b.run(True)
+        outs.append([b.get(f) for f in (C.FIELD_X, C.FIELD_PY, C.FIELD_STEPS)])
+    for o in outs[1:]:
+        for a, w in zip(o, outs[0]):
+            assert_bitwise(a, w) if a.dtype == np.float64 else np.testing.assert_array_equal(a, w)
+    o = 0
+    for s in sets:
+        n = s["n_particles"]
+        want = plain(s, *(c[o:o + n] for c in coords), 0)
+        np.testing.assert_array_equal(outs[0][2][o:o + n], want[4])
+        o += n
+    with pytest.raises(C.HMError):
+        b.set_groups(9)
