@@ -505,7 +505,7 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    work = {}
+    prof_work = {}
 
     def timed(mode, n_steps, n_warm):
         for _ in range(n_warm):
@@ -526,7 +526,7 @@ def run_ours(args):
             executed += e
             flops += f
         kernel_ms, launches = C.get_profile()
-        work["list_particles"], work["chunk_turns"] = C.get_profile_work()
+        prof_work["list_particles"], prof_work["chunk_turns"] = C.get_profile_work()
         C.set_profiling(False)
         barrier()
         return total_ms, executed, flops, kernel_ms, launches
@@ -537,7 +537,7 @@ def run_ours(args):
     # Bytes per launch: algorithmic (36 B in + 36 B out per list particle,
     # 32 B of records per turn) and DRAM traffic scaled from an ncu capture
     # of the same kernel (NCU_BYTES_PER_LIST_PARTICLE).
-    lp, ct = work["list_particles"], work["chunk_turns"]
+    lp, ct = prof_work["list_particles"], prof_work["chunk_turns"]
     algo_bytes = (72.0 * lp + 32.0 * ct) / launches if launches else None
     traffic = (NCU_BYTES_PER_LIST_PARTICLE * lp + 32.0 * ct) / launches if launches else None
 

@@ -68,35 +68,43 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     a.steps[i] = steps;
 }
 
-// v -= mean(v) per particle and coordinate; the mean is the left-to-right
-// sum from 0.0 divided by the sample count (std::accumulate / size).
+// v -= mean(v) per particle and coordinate, one thread per (particle,
+// coordinate); the mean is the left-to-right sum from 0.0 divided by the
+// sample count (std::accumulate / size).
 __global__ void mean_remove_kernel(double *x, double *px, double *y, double *py, size_t n,
                                    size_t S) {
-    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t i = t >> 2;
     if (i >= n) return;
-    double *c[4] = {x, px, y, py};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        double s = 0.0;
-        for (size_t k = 0; k < S; ++k) s = Rn::add(s, c[q][k * n + i]);
-        const double m = Rn::div(s, double(S));
-        for (size_t k = 0; k < S; ++k) c[q][k * n + i] = Rn::sub(c[q][k * n + i], m);
-    }
+    double *c = (t & 3u) == 0u ? x : (t & 3u) == 1u ? px : (t & 3u) == 2u ? y : py;
+    double s = 0.0;
+#pragma unroll 8
+    for (size_t k = 0; k < S; ++k) s = Rn::add(s, c[k * n + i]);
+    const double m = Rn::div(s, double(S));
+#pragma unroll 8
+    for (size_t k = 0; k < S; ++k) c[k * n + i] = Rn::sub(c[k * n + i], m);
 }
 
 // Birkhoff tune over samples [from, to] of (q, p): 1 - sum_i w_i dtheta_i /
 // (2 pi), dtheta wrapped by +2pi when negative, w = birkhoff_weights(to -
 // from); NaN when check_nan and any sample of the window is NaN.
-__device__ double birkhoff_window(const double *q, const double *p, size_t n, size_t i,
-                                  uint32_t from, uint32_t to, const double *w, bool check_nan,
-                                  bool *has_nan) {
+// Birkhoff tune of one plane over samples [from, to] of particle i; *has_nan
+// reports a NaN in any of the four coordinates of the window (q, p of this
+// plane and o1, o2 of the other).  The sample loads do not depend on the
+// running sum, so the loop is unrolled to keep several in flight.
+__device__ double birkhoff_window(const double *q, const double *p, const double *o1,
+                                  const double *o2, size_t n, size_t i, uint32_t from,
+                                  uint32_t to, const double *w, bool *has_nan) {
     double sum = 0.0;
     bool nan_seen = false;
-    double prev = atan2(p[size_t(from) * n + i], q[size_t(from) * n + i]);
-    nan_seen |= isnan(q[size_t(from) * n + i]) || isnan(p[size_t(from) * n + i]);
+    const size_t f = size_t(from) * n + i;
+    double prev = atan2(p[f], q[f]);
+    nan_seen |= isnan(q[f]) || isnan(p[f]) || isnan(o1[f]) || isnan(o2[f]);
+#pragma unroll 4
     for (uint32_t s = from; s < to; ++s) {
-        const double qq = q[size_t(s + 1) * n + i], pp = p[size_t(s + 1) * n + i];
-        nan_seen |= isnan(qq) || isnan(pp);
+        const size_t o = size_t(s + 1) * n + i;
+        const double qq = q[o], pp = p[o];
+        nan_seen |= isnan(qq) || isnan(pp) || isnan(o1[o]) || isnan(o2[o]);
         const double th = atan2(pp, qq);
         double d = Rn::sub(th, prev);
         if (d < 0.0) d = Rn::add(d, 2.0 * M_PI);
@@ -104,28 +112,28 @@ __device__ double birkhoff_window(const double *q, const double *p, size_t n, si
         prev = th;
     }
     *has_nan = nan_seen;
-    (void)check_nan;
     return Rn::sub(1.0, Rn::div(sum, Rn::mul(2.0, M_PI)));
 }
 
+// One thread per (particle, window, plane): for few particles the windows
+// and planes supply the parallelism.
 __global__ void birkhoff_kernel(const double *x, const double *px, const double *y,
                                 const double *py, size_t n, const uint32_t *from,
                                 const uint32_t *to, const uint64_t *w_off, const double *w,
                                 int n_win, double *out) {
-    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t i = t / (2u * size_t(n_win));
     if (i >= n) return;
-    const int cols = 2 * n_win;
-    for (int j = 0; j < n_win; ++j) {
-        bool nx = false, ny = false;
-        double tx = birkhoff_window(x, px, n, i, from[j], to[j], w + w_off[j], true, &nx);
-        double ty = birkhoff_window(y, py, n, i, from[j], to[j], w + w_off[j], true, &ny);
-        // birkhoff_tune_vec checks all four coordinates of the window for
-        // the windows it was given, not for the appended full orbit.
-        const bool is_full = j == n_win - 1;
-        if (!is_full && (nx || ny)) tx = ty = dev::quiet_nan();
-        out[i * cols + 2 * j] = tx;
-        out[i * cols + 2 * j + 1] = ty;
-    }
+    const int j = int((t / 2u) % size_t(n_win));
+    const bool plane_y = (t & 1u) != 0u;
+    bool nan_seen = false;
+    double tune = plane_y ? birkhoff_window(y, py, x, px, n, i, from[j], to[j], w + w_off[j], &nan_seen)
+                          : birkhoff_window(x, px, y, py, n, i, from[j], to[j], w + w_off[j], &nan_seen);
+    // birkhoff_tune_vec checks all four coordinates of the window for the
+    // windows it was given, not for the appended full orbit.
+    const bool is_full = j == n_win - 1;
+    if (!is_full && nan_seen) tune = dev::quiet_nan();
+    out[i * size_t(2 * n_win) + 2 * size_t(j) + (plane_y ? 1u : 0u)] = tune;
 }
 
 // z_k = (x + i px)[from + k] * 2 sin^2(pi k / len) for one window, one row
@@ -233,7 +241,7 @@ cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s) {
 cudaError_t launch_mean_remove(double *x, double *px, double *y, double *py, size_t n, size_t S,
                                cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    mean_remove_kernel<<<unsigned((n + 127) / 128), 128, 0, s>>>(x, px, y, py, n, S);
+    mean_remove_kernel<<<unsigned((4u * n + 127) / 128), 128, 0, s>>>(x, px, y, py, n, S);
     return cudaGetLastError();
 }
 
@@ -242,8 +250,9 @@ cudaError_t launch_birkhoff_tunes(const double *x, const double *px, const doubl
                                   const uint32_t *to, const uint64_t *w_off, const double *w,
                                   int n_win, double *out, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    birkhoff_kernel<<<unsigned((n + 127) / 128), 128, 0, s>>>(x, px, y, py, n, from, to, w_off,
-                                                              w, n_win, out);
+    const size_t threads = n * 2u * size_t(n_win);
+    birkhoff_kernel<<<unsigned((threads + 127) / 128), 128, 0, s>>>(x, px, y, py, n, from, to,
+                                                                    w_off, w, n_win, out);
     return cudaGetLastError();
 }
 
