@@ -68,15 +68,16 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     a.steps[i] = steps;
 }
 
-// v -= mean(v) per particle and coordinate, one thread per (particle,
-// coordinate); the mean is the left-to-right sum from 0.0 divided by the
-// sample count (std::accumulate / size).
+// v -= mean(v) per particle and coordinate, one thread per (coordinate,
+// particle), particles fastest; the mean is the left-to-right sum from 0.0
+// divided by the sample count (std::accumulate / size).
 __global__ void mean_remove_kernel(double *x, double *px, double *y, double *py, size_t n,
                                    size_t S) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const size_t i = t >> 2;
-    if (i >= n) return;
-    double *c = (t & 3u) == 0u ? x : (t & 3u) == 1u ? px : (t & 3u) == 2u ? y : py;
+    const size_t q = t / n;  // coordinate
+    if (q >= 4u) return;
+    const size_t i = t - q * n;
+    double *c = q == 0u ? x : q == 1u ? px : q == 2u ? y : py;
     double s = 0.0;
 #pragma unroll 8
     for (size_t k = 0; k < S; ++k) s = Rn::add(s, c[k * n + i]);
@@ -115,17 +116,20 @@ __device__ double birkhoff_window(const double *q, const double *p, const double
     return Rn::sub(1.0, Rn::div(sum, Rn::mul(2.0, M_PI)));
 }
 
-// One thread per (particle, window, plane): for few particles the windows
-// and planes supply the parallelism.
+// One thread per (window, plane, particle), particles fastest: a warp
+// walks one window of one plane for 32 consecutive particles (coalesced
+// loads, no divergence between windows of different lengths), and for few
+// particles the windows and planes supply the parallelism.
 __global__ void birkhoff_kernel(const double *x, const double *px, const double *y,
                                 const double *py, size_t n, const uint32_t *from,
                                 const uint32_t *to, const uint64_t *w_off, const double *w,
                                 int n_win, double *out) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const size_t i = t / (2u * size_t(n_win));
-    if (i >= n) return;
-    const int j = int((t / 2u) % size_t(n_win));
-    const bool plane_y = (t & 1u) != 0u;
+    const size_t wp = t / n;  // window * 2 + plane
+    if (wp >= 2u * size_t(n_win)) return;
+    const size_t i = t - wp * n;
+    const int j = int(wp >> 1);
+    const bool plane_y = (wp & 1u) != 0u;
     bool nan_seen = false;
     double tune = plane_y ? birkhoff_window(y, py, x, px, n, i, from[j], to[j], w + w_off[j], &nan_seen)
                           : birkhoff_window(x, px, y, py, n, i, from[j], to[j], w + w_off[j], &nan_seen);
