@@ -165,9 +165,12 @@ __device__ __forceinline__ bool turns_staged(const TrackChunk &c, const Barrier 
             issue(st + 2);
         }
     }
-    // A copy still in flight (issued for stage st + 1) must land before the
-    // block's shared memory is released.
-    if (st + 1 < n_stages && !timed_out) {
+    // Copies still in flight must land before the block's shared memory is
+    // released: the one issued for stage st + 1 and, after a wait that gave
+    // up, the one of stage st itself.  These waits are bounded too.
+    const bool gave_up = __syncthreads_or(timed_out);
+    if (gave_up && st < n_stages) dev::mbar_wait(&full[st & 1u], (st >> 1) & 1u);
+    if (st + 1 < n_stages) {
         const uint32_t nx = st + 1;
         if (!dev::mbar_wait(&full[nx & 1u], (nx >> 1) & 1u)) timed_out = true;
     }
