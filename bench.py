@@ -158,7 +158,7 @@ class ClockSampler:
                     reasons.add(name)
         if not mhz:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxs),
+        return {"sm_mhz": statistics.median(mhz), "sm_min_mhz": min(mhz), "sm_max_mhz": max(maxs),
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
@@ -387,7 +387,7 @@ def bench_tunes(C, turns=10_000, side=128):
         return time.perf_counter() - t0, b
 
     run()
-    dt, b = run()
+    dt, b = min((run() for _ in range(3)), key=lambda r: r[0])
     orbit_bytes = 32.0 * n * (turns + 1)
     return {"workload": f"{side}x{side} grid on [0,0.5]^2, eps 16, mu 0.2, {turns} turns, "
                         "orbit recorded, mean removed, Birkhoff + FFT tunes of 3 windows "
@@ -395,7 +395,8 @@ def bench_tunes(C, turns=10_000, side=128):
             "seconds": dt, "nominal_particle_turns_per_s": n * turns / dt,
             "orbit_bytes": orbit_bytes, "orbit_gb_per_s": orbit_bytes / dt / 1e9,
             "finite_tunes": int(np.isfinite(b).sum()),
-            "timing": "wall clock around one synchronous call (record + tunes)"}
+            "timing": "wall clock around one synchronous call (record + tunes), best of 3 "
+                      "after one warm-up"}
 
 
 def run_only(args):
@@ -585,24 +586,39 @@ def run_ours(args):
         pinned = [torch.from_numpy(a).pin_memory().numpy() for a in (x0, px0, y0, py0)]
         out_steps = torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
 
+        phase_s = {"create": 0.0, "track": 0.0, "get": 0.0, "destroy": 0.0}
+
         def e2e_step():
             for eps in EPSILONS:
                 for mu in MUS:
+                    t0 = time.perf_counter()
                     p = C.Particles(*pinned)
+                    t1 = time.perf_counter()
                     p_tr = trackers[eps]
                     p_tr.arith = arith
                     p_tr.track(p, args.turns, mu, BARRIER)
+                    t2 = time.perf_counter()
                     C.call("hm_particles_get", p.h, C.FIELD_STEPS,
                            out_steps.ctypes.data_as(C.c_void_p))
+                    t3 = time.perf_counter()
                     del p
+                    t4 = time.perf_counter()
+                    for k, dt in zip(phase_s, (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
+                        phase_s[k] += dt
 
         e2e_step()
         barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
+        for k in phase_s:
+            phase_s[k] = 0.0
+        C.set_profiling(True)
+        with ClockSampler(local) as e2e_clocks:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step()
+            torch.cuda.synchronize()
+            e2e_s = time.perf_counter() - t0
+        e2e_kernel_ms, _ = C.get_profile()
+        C.set_profiling(False)
         if dist is not None:
             t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -610,6 +626,10 @@ def run_ours(args):
         e2e = {"value": float(n) * args.turns * 6 * world * args.steps / e2e_s, "unit": UNIT,
                "steps": args.steps,
                "h2d_bytes_per_step": 6 * 4 * 8 * n, "d2h_bytes_per_step": 6 * 4 * n,
+               "ms_per_step": e2e_s * 1e3 / args.steps,
+               "kernel_ms_per_step": e2e_kernel_ms / args.steps,
+               "phase_ms_per_step": {k: v * 1e3 / args.steps for k, v in phase_s.items()},
+               "clocks": e2e_clocks.summary(),
                "path": "hm_particles_create (pinned host) -> hm_track -> hm_particles_get(steps)"}
 
     cpu = None

@@ -99,6 +99,7 @@ _SIGNATURES = {
                                        c_size_t, c_void_p, c_uint64, c_uint32, c_uint32,
                                        c_double, c_double, c_int, c_int, c_void_p]),
     "hm_fp64_peak": (None, [c_double, _PD, _PD]),
+    "hm_release_cached_memory": (None, []),
     "hm_set_profiling": (None, [c_int]),
     "hm_get_profile": (None, [_PD, POINTER(c_uint64)]),
     "hm_get_profile_work": (None, [c_void_p, c_void_p]),
@@ -709,6 +710,11 @@ def get_profile_work():
     a, b = c_uint64(), c_uint64()
     call("hm_get_profile_work", ctypes.byref(a), ctypes.byref(b))
     return int(a.value), int(b.value)
+
+
+def release_cached_memory() -> None:
+    """Returns the unused blocks of the library's device memory pools."""
+    call("hm_release_cached_memory")
 
 
 def set_profiling(on: bool) -> None:

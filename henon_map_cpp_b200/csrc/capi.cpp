@@ -112,11 +112,65 @@ bool cancel_requested() {
 
 // ---- device buffers ---------------------------------------------------------------
 
+namespace {
+
+// One pool per device, created on first use.  Its release threshold is
+// unlimited: blocks freed into it stay mapped and are handed out again,
+// until hm_release_cached_memory trims it.
+struct PoolTable {
+    std::mutex mutex;
+    std::vector<cudaMemPool_t> pools;  // by device ordinal; null until first use
+};
+
+PoolTable &pool_table() {
+    static PoolTable t;
+    return t;
+}
+
+hm_status device_pool(int dev, cudaMemPool_t *out) {
+    PoolTable &t = pool_table();
+    std::lock_guard<std::mutex> lock(t.mutex);
+    if (t.pools.size() <= size_t(dev)) t.pools.resize(size_t(dev) + 1, nullptr);
+    if (!t.pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        HM_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep_all = UINT64_MAX;
+        const cudaError_t e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return cuda_fail(e, "cudaMemPoolSetAttribute");
+        }
+        t.pools[dev] = pool;
+    }
+    *out = t.pools[dev];
+    return ok();
+}
+
+// Makes dev current for the lifetime of the guard.
+struct DeviceGuard {
+    int saved = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&saved) == cudaSuccess && saved != dev) cudaSetDevice(dev);
+        else saved = -1;
+    }
+    ~DeviceGuard() {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
+
+}  // namespace
+
 DeviceBuffer &DeviceBuffer::operator=(DeviceBuffer &&o) noexcept {
     if (this != &o) {
         release();
         ptr = o.ptr;
         bytes = o.bytes;
+        device = o.device;
         o.ptr = nullptr;
         o.bytes = 0;
     }
@@ -126,7 +180,13 @@ DeviceBuffer &DeviceBuffer::operator=(DeviceBuffer &&o) noexcept {
 DeviceBuffer::~DeviceBuffer() { release(); }
 
 void DeviceBuffer::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        // As cudaFree: every use of the block, on any stream, ends before
+        // the pool may hand it out again.
+        DeviceGuard guard(device);
+        cudaDeviceSynchronize();
+        cudaFreeAsync(ptr, 0);
+    }
     ptr = nullptr;
     bytes = 0;
 }
@@ -134,8 +194,57 @@ void DeviceBuffer::release() {
 hm_status DeviceBuffer::alloc(size_t nbytes) {
     release();
     if (nbytes == 0) return ok();
-    HM_CUDA_TRY(cudaMalloc(&ptr, nbytes));
+    int dev = 0;
+    HM_CUDA_TRY(cudaGetDevice(&dev));
+    cudaMemPool_t pool = nullptr;
+    HM_TRY(device_pool(dev, &pool));
+    void *p = nullptr;
+    cudaError_t got = cudaMallocFromPoolAsync(&p, nbytes, pool, 0);
+    if (got == cudaErrorMemoryAllocation) {
+        // Blocks the pool keeps but does not use may be what is missing:
+        // hand them back to the device and try once more.
+        cudaGetLastError();
+        HM_CUDA_TRY(cudaDeviceSynchronize());
+        HM_CUDA_TRY(cudaMemPoolTrimTo(pool, 0));
+        got = cudaMallocFromPoolAsync(&p, nbytes, pool, 0);
+    }
+    if (got != cudaSuccess) return cuda_fail(got, "cudaMallocFromPoolAsync");
+    // The block is ordered on the legacy stream; waiting for it makes it
+    // usable from every stream, like a cudaMalloc block.
+    const cudaError_t e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(p, 0);
+        return cuda_fail(e, "cudaStreamSynchronize after pool allocation");
+    }
+    ptr = p;
     bytes = nbytes;
+    device = dev;
+    return ok();
+}
+
+hm_status device_free_bytes(size_t *free_bytes) {
+    size_t free_b = 0, total_b = 0;
+    HM_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    int dev = 0;
+    HM_CUDA_TRY(cudaGetDevice(&dev));
+    cudaMemPool_t pool = nullptr;
+    HM_TRY(device_pool(dev, &pool));
+    uint64_t reserved = 0, used = 0;
+    HM_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    HM_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    *free_bytes = free_b + size_t(reserved > used ? reserved - used : 0);
+    return ok();
+}
+
+hm_status release_cached_memory() {
+    PoolTable &t = pool_table();
+    std::lock_guard<std::mutex> lock(t.mutex);
+    for (size_t d = 0; d < t.pools.size(); ++d) {
+        if (!t.pools[d]) continue;
+        DeviceGuard guard(static_cast<int>(d));
+        HM_CUDA_TRY(cudaDeviceSynchronize());
+        HM_CUDA_TRY(cudaMemPoolTrimTo(t.pools[d], 0));
+    }
     return ok();
 }
 
@@ -437,28 +546,68 @@ namespace hm {
 // (Re)allocates the device arrays of p for p->n_total particles and uploads
 // coordinates, steps and the host-side bookkeeping vectors.
 hm_status particles_upload(hm_particles *p, const double *x, const double *px,
-                           const double *y, const double *py,
-                           const std::vector<uint32_t> &steps) {
+                           const double *y, const double *py) {
     const size_t n = p->n_total;
-    hm::DeviceBuffer *dbl[4] = {&p->x, &p->px, &p->y, &p->py};
+    hm::DeviceBuffer *cur[4] = {&p->x, &p->px, &p->y, &p->py};
+    hm::DeviceBuffer *ini[4] = {&p->x0d, &p->px0d, &p->y0d, &p->py0d};
     const double *src[4] = {x, px, y, py};
     for (int f = 0; f < 4; ++f) {
-        HM_TRY(dbl[f]->alloc(n * sizeof(double)));
-        if (n) HM_CUDA_TRY(cudaMemcpy(dbl[f]->ptr, src[f], n * sizeof(double), cudaMemcpyHostToDevice));
+        HM_TRY(cur[f]->alloc(n * sizeof(double)));
+        HM_TRY(ini[f]->alloc(n * sizeof(double)));
     }
     HM_TRY(p->steps.alloc(n * sizeof(uint32_t)));
     HM_TRY(p->dvalid.alloc(n));
     HM_TRY(p->dghost.alloc(n));
     HM_TRY(p->didx.alloc(n * sizeof(uint64_t)));
     HM_TRY(p->didx_base.alloc(n * sizeof(uint64_t)));
-    if (n) {
-        HM_CUDA_TRY(cudaMemcpy(p->steps.ptr, steps.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        HM_CUDA_TRY(cudaMemcpy(p->dvalid.ptr, p->valid.data(), n, cudaMemcpyHostToDevice));
-        HM_CUDA_TRY(cudaMemcpy(p->dghost.ptr, p->ghost.data(), n, cudaMemcpyHostToDevice));
-        HM_CUDA_TRY(cudaMemcpy(p->didx.ptr, p->idx.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice));
-        HM_CUDA_TRY(cudaMemcpy(p->didx_base.ptr, p->idx_base.data(), n * sizeof(uint64_t),
-                               cudaMemcpyHostToDevice));
+    if (n == 0) return ok();
+    const cudaStream_t s = 0;
+    for (int f = 0; f < 4; ++f) {
+        HM_CUDA_TRY(cudaMemcpyAsync(cur[f]->ptr, src[f], n * sizeof(double), cudaMemcpyHostToDevice, s));
+        HM_CUDA_TRY(cudaMemcpyAsync(ini[f]->ptr, cur[f]->ptr, n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, s));
     }
+    HM_CUDA_TRY(cudaMemsetAsync(p->steps.ptr, 0, n * sizeof(uint32_t), s));
+    if (p->host_ready) {
+        HM_CUDA_TRY(cudaMemcpyAsync(p->dvalid.ptr, p->valid.data(), n, cudaMemcpyHostToDevice, s));
+        HM_CUDA_TRY(cudaMemcpyAsync(p->dghost.ptr, p->ghost.data(), n, cudaMemcpyHostToDevice, s));
+        HM_CUDA_TRY(cudaMemcpyAsync(p->didx.ptr, p->idx.data(), n * sizeof(uint64_t),
+                                    cudaMemcpyHostToDevice, s));
+        HM_CUDA_TRY(cudaMemcpyAsync(p->didx_base.ptr, p->idx_base.data(), n * sizeof(uint64_t),
+                                    cudaMemcpyHostToDevice, s));
+    } else {
+        HM_CUDA_TRY(cudaMemsetAsync(p->dvalid.ptr, 1, n, s));
+        HM_CUDA_TRY(cudaMemsetAsync(p->dghost.ptr, 0, n, s));
+        HM_CUDA_TRY(launch_particle_indices(p->didx.as<uint64_t>(), p->didx_base.as<uint64_t>(), n, s));
+    }
+    // The caller's (possibly pinned) arrays and the mirrors must outlive the copies.
+    HM_CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
+}
+
+hm_status particles_host_mirror(const hm_particles *p) {
+    if (p->host_ready) return ok();
+    const size_t n = p->n_total;
+    p->x0.resize(n);
+    p->px0.resize(n);
+    p->y0.resize(n);
+    p->py0.resize(n);
+    p->valid.resize(n);
+    p->ghost.resize(n);
+    p->idx.resize(n);
+    p->idx_base.resize(n);
+    if (n) {
+        const hm::DeviceBuffer *ini[4] = {&p->x0d, &p->px0d, &p->y0d, &p->py0d};
+        std::vector<double> *dst[4] = {&p->x0, &p->px0, &p->y0, &p->py0};
+        for (int f = 0; f < 4; ++f)
+            HM_CUDA_TRY(cudaMemcpy(dst[f]->data(), ini[f]->ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+        HM_CUDA_TRY(cudaMemcpy(p->valid.data(), p->dvalid.ptr, n, cudaMemcpyDeviceToHost));
+        HM_CUDA_TRY(cudaMemcpy(p->ghost.data(), p->dghost.ptr, n, cudaMemcpyDeviceToHost));
+        HM_CUDA_TRY(cudaMemcpy(p->idx.data(), p->didx.ptr, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        HM_CUDA_TRY(cudaMemcpy(p->idx_base.data(), p->didx_base.ptr, n * sizeof(uint64_t),
+                               cudaMemcpyDeviceToHost));
+    }
+    p->host_ready = true;
     return ok();
 }
 
@@ -492,6 +641,8 @@ hm_status hm_set_track_config(int threads, int per_thread, uint32_t chunk0, uint
 }
 
 hm_status hm_set_track_staging(uint32_t stage_turns) { return hm::set_track_staging(stage_turns); }
+
+hm_status hm_release_cached_memory(void) { return hm::release_cached_memory(); }
 
 hm_status hm_get_track_staging(uint32_t *stage_turns) {
     if (!stage_turns) return fail(HM_ERR_INVALID_ARG, "null output");
@@ -639,16 +790,7 @@ hm_status hm_particles_create(const double *x, const double *px, const double *y
     if (n > 0xffffffffULL) return fail(HM_ERR_INVALID_ARG, "too many particles (max 2^32-1)");
     auto *p = new hm_particles();
     p->n_total = p->n_particles = n;
-    p->x0.assign(x, x + n);
-    p->px0.assign(px, px + n);
-    p->y0.assign(y, y + n);
-    p->py0.assign(py, py + n);
-    p->valid.assign(n, 1);
-    p->ghost.assign(n, 0);
-    p->idx.resize(n);
-    p->idx_base.resize(n);
-    for (size_t i = 0; i < n; ++i) p->idx[i] = p->idx_base[i] = i;
-    const hm_status s = particles_upload(p, x, px, y, py, std::vector<uint32_t>(n, 0u));
+    const hm_status s = particles_upload(p, x, px, y, py);
     if (s != HM_OK) {
         delete p;
         return s;
@@ -664,10 +806,24 @@ hm_status hm_particles_destroy(hm_particles *p) {
 
 hm_status hm_particles_reset(hm_particles *p) {
     if (!p) return fail(HM_ERR_INVALID_ARG, "null particles");
-    std::fill(p->valid.begin(), p->valid.end(), uint8_t(1));
+    // Restart from the initial conditions with steps = 0 and valid = 1
+    // (particles_4d::reset and particles_4d_gpu::reset,
+    // src/henon.cu:727-735, 1238-1244); ghosts and indices
+    // are unchanged.
+    if (p->host_ready) std::fill(p->valid.begin(), p->valid.end(), uint8_t(1));
     p->live_step = 0;
-    return particles_upload(p, p->x0.data(), p->px0.data(), p->y0.data(), p->py0.data(),
-                            std::vector<uint32_t>(p->n_total, 0u));
+    const size_t n = p->n_total;
+    if (n == 0) return ok();
+    const cudaStream_t s = 0;
+    const hm::DeviceBuffer *ini[4] = {&p->x0d, &p->px0d, &p->y0d, &p->py0d};
+    hm::DeviceBuffer *cur[4] = {&p->x, &p->px, &p->y, &p->py};
+    for (int f = 0; f < 4; ++f)
+        HM_CUDA_TRY(cudaMemcpyAsync(cur[f]->ptr, ini[f]->ptr, n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, s));
+    HM_CUDA_TRY(cudaMemsetAsync(p->steps.ptr, 0, n * sizeof(uint32_t), s));
+    HM_CUDA_TRY(cudaMemsetAsync(p->dvalid.ptr, 1, n, s));
+    HM_CUDA_TRY(cudaStreamSynchronize(s));
+    return ok();
 }
 
 hm_status hm_particles_size(const hm_particles *p, size_t *n_total, size_t *n_particles,

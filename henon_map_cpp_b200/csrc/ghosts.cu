@@ -72,7 +72,23 @@ __global__ void displacement_kernel(const double *x, const double *px, const dou
     dpy[o] = Rn::sub(realign(gpy, bpy, ratio), bpy);
 }
 
+// idx = idx_base = i: the indices of a set without ghosts (particles_4d
+// constructor, src/henon.cu:713-719).
+__global__ void particle_indices_kernel(uint64_t *idx, uint64_t *idx_base, size_t n) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) {
+        idx[i] = i;
+        idx_base[i] = i;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_particle_indices(uint64_t *idx, uint64_t *idx_base, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    particle_indices_kernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(idx, idx_base, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_renormalize(double *x, double *px, double *y, double *py,
                                const uint64_t *idx_base, const uint8_t *ghost, size_t n,

@@ -50,14 +50,19 @@ hm_status modulation_ripple(const std::string &kind, uint32_t n_turns, double om
 
 // ---- device buffers ---------------------------------------------------------
 
-// Owning device allocation (cudaMalloc / cudaFree), move-only.
+// Owning device allocation, move-only.  Blocks come from a per-device
+// memory pool that keeps freed blocks for reuse (capi.cpp), so creating
+// and destroying particle sets, trackers and scratch in a loop makes no
+// allocation or unmapping call into the driver once the pool has grown.
+// release() waits for the device like cudaFree before the block is reused.
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
+    int device = 0;
     DeviceBuffer() = default;
     DeviceBuffer(const DeviceBuffer &) = delete;
     DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-    DeviceBuffer(DeviceBuffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    DeviceBuffer(DeviceBuffer &&o) noexcept : ptr(o.ptr), bytes(o.bytes), device(o.device) {
         o.ptr = nullptr;
         o.bytes = 0;
     }
@@ -68,6 +73,10 @@ struct DeviceBuffer {
     void release();
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
+
+// Free device memory of the current device, counting the blocks that the
+// library's pool holds but does not use (capi.cpp).
+hm_status device_free_bytes(size_t *free_bytes);
 
 }  // namespace hm
 
@@ -83,11 +92,18 @@ struct hm_particles {
     // start at 0, survivors advance together and lost ones are frozen as NaN,
     // so the table index of a whole track() call is uniform.
     uint32_t live_step = 0;
-    // Host copies of what the reference keeps on the host side.
-    std::vector<double> x0, px0, y0, py0;
-    std::vector<uint8_t> valid, ghost;
-    std::vector<uint64_t> idx, idx_base;
+    // Device state, and the initial conditions on the device (reset
+    // restarts from them).  The device copies are authoritative.
     hm::DeviceBuffer x, px, y, py, steps, dvalid, dghost, didx, didx_base;
+    hm::DeviceBuffer x0d, px0d, y0d, py0d;
+    // Host mirrors of what the reference keeps on the host side (initial
+    // conditions, valid, ghost, idx, idx_base).  Built from the device
+    // copies on first use (add_ghost, tangent matrices), so that creating
+    // and tracking a set never touches host memory beyond the caller's.
+    mutable bool host_ready = false;
+    mutable std::vector<double> x0, px0, y0, py0;
+    mutable std::vector<uint8_t> valid, ghost;
+    mutable std::vector<uint64_t> idx, idx_base;
     hm::DeviceBuffer work;  // survivor lists of the chunked tracker
     // Generator of "random" ghost directions: default-seeded, one per
     // particle set, as the reference's particles_4d::rng.
@@ -361,11 +377,17 @@ cudaError_t launch_hann_gather(const double *q, const double *p, size_t n, uint3
 cudaError_t launch_fft_peak(const double2 *buf, uint32_t len, size_t count, const int *nan_flags,
                             double *out, size_t out_stride, size_t first, cudaStream_t s);
 
-// (Re)allocates and uploads the device arrays of p (capi.cpp).
+// (Re)allocates the device arrays of p's n_total particles and starts them
+// at the given host coordinates, which become the initial conditions:
+// steps = 0 and valid = 1; ghost, idx and idx_base from the host mirrors
+// when they are built, else those of a set without ghosts (capi.cpp).
 hm_status particles_upload(hm_particles *p, const double *x, const double *px, const double *y,
-                           const double *py, const std::vector<uint32_t> &steps);
+                           const double *py);
+// Builds p's host mirrors from the device copies, once (capi.cpp).
+hm_status particles_host_mirror(const hm_particles *p);
 
-// Ghost particles (ghosts.cu).
+// Ghost particles and particle indices (ghosts.cu).
+cudaError_t launch_particle_indices(uint64_t *idx, uint64_t *idx_base, size_t n, cudaStream_t s);
 cudaError_t launch_renormalize(double *x, double *px, double *y, double *py,
                                const uint64_t *idx_base, const uint8_t *ghost, size_t n,
                                double module, cudaStream_t s);

@@ -90,6 +90,7 @@ hm_status hm_particles_add_ghost(hm_particles *p, double module, const char *dir
     const std::string dir(direction);
     if (dir != "x" && dir != "px" && dir != "y" && dir != "py" && dir != "random")
         return fail(HM_ERR_INVALID_ARG, "Invalid direction.");
+    HM_TRY(hm::particles_host_mirror(p));
     const size_t n = p->n_total;
     std::vector<double> gx, gpx, gy, gpy;
     std::vector<uint8_t> gvalid;
@@ -122,8 +123,7 @@ hm_status hm_particles_add_ghost(hm_particles *p, double module, const char *dir
     p->n_ghosts += 1;
     p->live_step = 0;
     p->work.release();
-    return hm::particles_upload(p, p->x0.data(), p->px0.data(), p->y0.data(), p->py0.data(),
-                                std::vector<uint32_t>(p->n_total, 0u));
+    return hm::particles_upload(p, p->x0.data(), p->px0.data(), p->y0.data(), p->py0.data());
 }
 
 // renormalize (src/henon.cu:1257-1282): every ghost moved along its
@@ -194,6 +194,7 @@ hm_status hm_tracker_tangent_matrices(const hm_tracker *t, const hm_particles *p
     const uint32_t s = p->global_steps;
     if (s >= t->allowed_steps)
         return fail(HM_ERR_BUDGET, "The number of turns is too large. (tangent matrix past the table end)");
+    HM_TRY(hm::particles_host_mirror(p));
     std::vector<double> x(n), px(n), y(n), py(n);
     HM_CUDA_TRY(cudaMemcpy(x.data(), p->x.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
     HM_CUDA_TRY(cudaMemcpy(px.data(), p->px.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));

@@ -184,8 +184,8 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
     const std::vector<uint32_t> f(from, from + n_windows), tt(to, to + n_windows);
     const size_t cols = 2 * (n_windows + 1);
     // Orbit slice: at most half the free device memory.
-    size_t free_b = 0, total_b = 0;
-    HM_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    size_t free_b = 0;
+    HM_TRY(hm::device_free_bytes(&free_b));
     const size_t per_particle = S * 4 * sizeof(double);
     const size_t slice = std::max<size_t>(1, std::min<size_t>(n, (free_b / 2) / per_particle));
     DeviceBuffer orbit, out;

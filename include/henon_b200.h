@@ -515,6 +515,16 @@ hm_status hm_track_device_noalloc(double *x, double *px, double *y, double *py,
                                   double mu, double barrier, int inverse,
                                   hm_arith arith, void *stream);
 
+/* ---- device memory ----------------------------------------------------- */
+
+/* The library's device buffers (particles, tables, scratch) come from one
+ * memory pool per device that keeps freed blocks for reuse, so a loop that
+ * creates and destroys particle sets makes no allocation call into the
+ * driver once the pool has grown.  This returns the pool's unused blocks
+ * to the device (cf. torch.cuda.empty_cache); buffers in use are kept.
+ * Waits for every device the library has allocated on. */
+hm_status hm_release_cached_memory(void);
+
 /* ---- measurement ------------------------------------------------------- */
 
 /* Times every tracking kernel launch with CUDA events on its stream while
