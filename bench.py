@@ -217,7 +217,7 @@ def bench_batched(C, arith):
 
     sets, coords = sweep.heterogeneous_sets(seed=20261203)
     b = C.Batch(sets)
-    b.configure(arith, 1, 512, 16384)
+    b.configure(arith, 1, 512, 4096)
     b.load(*coords)
     b.run(True)  # capture + warm-up
     times = []
@@ -227,13 +227,16 @@ def bench_batched(C, arith):
         times.append(time.perf_counter() - t0)
     t_batch = min(times)
     steps_batch = b.get(C.FIELD_STEPS)
-    # the same batch tracked as one group (no overlap of chunk ramp-downs)
+    # the same batch tracked as one group on the whole device (no overlap of
+    # chunk ramp-downs)
     b.set_groups(1)
+    b.set_grid_share(0.0)
     b.run(True)
     t0 = time.perf_counter()
     b.run(True)
     t_one_group = time.perf_counter() - t0
-    b.set_groups(4)
+    b.set_groups(8)
+    b.set_grid_share(1.5)
     # plain: one chunked tracking call per set on device arrays
     t_plain, equal, o = 0.0, True, 0
     stream = torch.cuda.current_stream().cuda_stream

@@ -166,6 +166,7 @@ _SIGNATURES = {
     "hm_batch_destroy": (None, [c_void_p]),
     "hm_batch_configure": (None, [c_void_p, c_int, c_int, c_uint32, c_uint32]),
     "hm_batch_set_groups": (None, [c_void_p, c_int]),
+    "hm_batch_set_grid_share": (None, [c_void_p, c_double]),
     "hm_batch_size": (None, [c_void_p, POINTER(c_uint64), POINTER(c_uint32)]),
     "hm_batch_load": (None, [c_void_p, _PD, _PD, _PD, _PD]),
     "hm_batch_run": (None, [c_void_p, c_int]),
@@ -632,6 +633,11 @@ class Batch(_Handle):
     def set_groups(self, groups: int) -> None:
         """Number of concurrently tracked groups of sets (1..8)."""
         call("hm_batch_set_groups", self.h, int(groups))
+
+    def set_grid_share(self, share: float) -> None:
+        """Grid of each group's chunk kernel, as share x the group's fraction of
+        the work of the whole device (0: every group spans the device)."""
+        call("hm_batch_set_grid_share", self.h, float(share))
 
     def n_chunks(self) -> int:
         a, b = c_uint64(), c_uint32()

@@ -39,8 +39,9 @@ def _current_shape() -> dict:
     shape = dict(zip(("threads", "per_thread", "chunk0", "chunk_max"), C.get_track_config()))
     shape["stage_turns"] = C.get_track_staging()
     return shape
-BATCH_SPACE = {"groups": (4, 1, 2, 8), "per_thread": (1, 2, 4), "chunk0": (256, 512, 1024),
-               "chunk_max": (8192, 16384)}
+BATCH_SPACE = {"groups": (8, 4, 2, 1), "grid_share": (1.5, 1.0, 2.0, 0.0),
+               "per_thread": (1, 2, 4), "chunk0": (256, 512, 1024),
+               "chunk_max": (4096, 8192, 16384)}
 
 
 def _device_name() -> str:
@@ -122,17 +123,18 @@ def tune_batch(sets, coords, arith: int = C.ARITH_EXACT, budget_s: float = 30.0)
     res = {}
     start = time.perf_counter()
     groups = None
-    for g, k, c0, cm in itertools.product(*BATCH_SPACE.values()):
+    for g, share, k, c0, cm in itertools.product(*BATCH_SPACE.values()):
         if cm < c0 or time.perf_counter() - start > budget_s:
             continue
         if g != groups:
             b.set_groups(g)
             groups = g
+        b.set_grid_share(share)
         b.configure(arith, k, c0, cm)
         b.run(True)
         t0 = time.perf_counter()
         b.run(True)
-        res[(g, k, c0, cm)] = time.perf_counter() - t0
+        res[(g, share, k, c0, cm)] = time.perf_counter() - t0
     best = min(res, key=res.get)
     return dict(zip(BATCH_SPACE, best)), res[best], {str(k): v for k, v in res.items()}
 

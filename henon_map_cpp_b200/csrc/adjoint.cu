@@ -78,9 +78,9 @@ __device__ __forceinline__ void rec_store(double *buf, const double (&r)[kPerThr
 template <int ARITH, bool OCT>
 __device__ __forceinline__ double fwd(S4 &s, const dev::Turn &t, double mu) {
     dev::Particle p = dev::make_particle(s.x, s.px, s.y, s.py);
-    const double r = dev::turn<ARITH, OCT, false>(p, t, mu);
+    dev::turn<ARITH, OCT, false>(p, t, mu);
     s = S4{p.x, p.px, p.y, p.py};
-    return ARITH == HM_ARITH_EXACT ? dev::radius_exact(p) : r;
+    return ARITH == HM_ARITH_EXACT ? dev::radius_exact(p) : dev::radius_fma(p);
 }
 
 __device__ __forceinline__ void store4(double *buf, size_t slot, size_t n, size_t i, const S4 &s) {

@@ -21,6 +21,14 @@ using hm::ok;
 // ramp-down is filled by another group's tiles instead of idling until the
 // next chunk.  The set metadata is stored group by group (position order);
 // particles keep the caller's order.
+//
+// Each group's persistent chunk kernel gets a share of the device's resident
+// blocks in proportion to the group's work, grid_share x (its particles x
+// turns) / (all of them), at most the whole device.  Several groups'
+// kernels then run side by side, each with more rounds of tiles per launch
+// than one kernel spread over the whole device, so less of each launch is
+// spent in its last, partly empty round; a group heavier than the others
+// (one large set) still gets a proportionally larger grid.
 struct hm_batch {
     std::vector<hm_batch_set> params;  // caller's order
     std::vector<std::string> kinds;
@@ -34,7 +42,8 @@ struct hm_batch {
     hm::BatchDev dev{};  // all sets (reset and collection)
     int arith = HM_ARITH_EXACT;
     int per_thread = 1;
-    uint32_t chunk0 = 512, chunk_max = 16384;
+    uint32_t chunk0 = 512, chunk_max = 4096;
+    double grid_share = 1.5;  // 0: every group's kernel spans the device
     int n_groups = 1;
     std::vector<uint32_t> order;        // position -> caller's set index
     std::vector<uint32_t> group_first;  // sets of group g: positions [first[g], first[g+1])
@@ -112,14 +121,28 @@ hm_status enqueue(hm_batch *b) {
     HM_CUDA_TRY(cudaMemsetAsync(b->state.ptr, 0, b->params.size() * sizeof(hm::BatchStateDev), s));
     HM_CUDA_TRY(hm::launch_batch_init(b->dev, s));
     HM_CUDA_TRY(cudaEventRecord(b->events[0], s));
+    std::vector<double> work(size_t(b->n_groups), 0.0);
+    double total = 0.0;
+    for (int g = 0; g < b->n_groups; ++g) {
+        for (uint32_t q = b->group_first[g]; q < b->group_first[g + 1]; ++q) {
+            const hm_batch_set &p = b->params[b->order[q]];
+            work[size_t(g)] += double(p.n_particles) * double(p.n_turns);
+        }
+        total += work[size_t(g)];
+    }
     for (int g = 0; g < b->n_groups; ++g) {
         const cudaStream_t gs = b->group_streams[size_t(g)];
         const hm::BatchDev d = b->group_dev(g);
+        int blocks = b->blocks;
+        if (b->grid_share > 0.0 && total > 0.0) {
+            const double share = b->grid_share * work[size_t(g)] / total;
+            blocks = std::max(1, std::min(b->blocks, int(std::ceil(share * b->blocks))));
+        }
         HM_CUDA_TRY(cudaStreamWaitEvent(gs, b->events[0], 0));
         uint32_t prev = 0;
         for (uint32_t len : b->schedule(b->group_turns(g))) {
             HM_CUDA_TRY(hm::launch_batch_plan(d, prev, len, gs));
-            HM_CUDA_TRY(hm::launch_batch_chunk(d, b->blocks, gs));
+            HM_CUDA_TRY(hm::launch_batch_chunk(d, blocks, gs));
             prev = len;
         }
         HM_CUDA_TRY(hm::launch_batch_plan(d, prev, 0, gs));
@@ -269,7 +292,7 @@ hm_status hm_batch_create(size_t n_sets, const hm_batch_set *sets, hm_batch **ou
         const cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) s = hm::cuda_fail(e, "cudaStreamCreate");
     }
-    if (s == HM_OK) s = layout(b, 4);
+    if (s == HM_OK) s = layout(b, kMaxGroups);
     if (s != HM_OK) {
         delete b;
         return s;
@@ -320,6 +343,16 @@ hm_status hm_batch_configure(hm_batch *b, hm_arith arith, int per_thread, uint32
     b->chunk_max = chunk_max;
     b->dev.arith = arith;
     b->dev.per_thread = per_thread;
+    b->blocks = 0;  // the resident-block count depends on the kernel variant
+    b->drop_graph();
+    return ok();
+}
+
+hm_status hm_batch_set_grid_share(hm_batch *b, double share) {
+    if (!b) return fail(HM_ERR_INVALID_ARG, "null batch");
+    if (!(share >= 0.0) || std::isinf(share))
+        return fail(HM_ERR_INVALID_ARG, "grid share must be finite and >= 0");
+    b->grid_share = share;
     b->drop_graph();
     return ok();
 }

@@ -127,6 +127,8 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
         id[j] = b.list_idx[in][slot];
         p[j] = dev::make_particle(b.list_x[in][slot], b.list_px[in][slot], b.list_y[in][slot],
                                   b.list_py[in][slot]);
+        // Slots without a live particle hold zeros, a fixed point of the map.
+        if (!live[j]) p[j] = dev::make_particle(0.0, 0.0, 0.0, 0.0);
         any |= live[j];
     }
     const uint32_t turn0 = st.done, nt = st.turns;
@@ -153,23 +155,24 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
             const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * kk);
             const double2 q0 = q[0], q1 = q[1];
             const dev::Turn t{q0.x, q0.y, q1.x, q1.y};
-            bool any_check = false;
-            bool check[K];
-            double r[K];
+            // Per thread one OR of the coordinates' high words and one
+            // compare; lost particles hold zeros (see track.cu turn_all).
+            uint32_t ored = 0u;
 #pragma unroll
             for (int j = 0; j < K; ++j) {
-                r[j] = dev::turn<ARITH, OCT, false>(p[j], t, mu);
-                check[j] = live[j] && !dev::surely_inside(r[j], bar);
-                any_check |= check[j];
+                dev::turn<ARITH, OCT, false>(p[j], t, mu);
+                ored |= dev::hi_or(p[j]);
             }
-            if (__any_sync(dev::kFullMask, any_check)) {
+            if (__any_sync(dev::kFullMask, !dev::small_or(ored, bar))) {
                 bool still = false;
 #pragma unroll
                 for (int j = 0; j < K; ++j) {
-                    if (check[j] && !dev::settle_inside<ARITH>(r[j], p[j], bar)) {
+                    if (live[j] && !dev::small_inside(p[j], bar) &&
+                        !dev::inside<ARITH>(dev::radius_fma(p[j]), p[j], bar)) {
                         b.x[id[j]] = b.px[id[j]] = b.y[id[j]] = b.py[id[j]] = dev::quiet_nan();
                         b.steps[id[j]] = turn0 + k;
                         live[j] = false;
+                        p[j] = dev::make_particle(0.0, 0.0, 0.0, 0.0);
                     }
                     still |= live[j];
                 }
@@ -211,9 +214,10 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
     }
 }
 
-// Persistent: warps pop warp-tiles until the chunk's queue is empty.
+// Persistent: warps pop warp-tiles until the chunk's queue is empty.  One
+// particle per thread fits 72 registers without spills: 7 blocks per SM.
 template <int ARITH, int K>
-__global__ void __launch_bounds__(kThreads) batch_chunk_kernel(BatchDev b) {
+__global__ void __launch_bounds__(kThreads, K == 1 ? 7 : 1) batch_chunk_kernel(BatchDev b) {
     __shared__ __align__(16) double stage_bufs[kWarps][2 * kStageTurns * 4];
     const unsigned lane = threadIdx.x & 31u;
     double *bufs = stage_bufs[threadIdx.x >> 5];

@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
         if (alive) {
             const dev::Turn t = dev::load_turn(a.table, a.live_step + k);
             dev::Particle q = dev::make_particle(x, px, y, py);
-            const double r = dev::turn<HM_ARITH_EXACT, OCT, false>(q, t, mu);
-            if (dev::inside<HM_ARITH_EXACT>(r, q, bar)) {
+            dev::turn<HM_ARITH_EXACT, OCT, false>(q, t, mu);
+            if (dev::inside_after_turn<HM_ARITH_EXACT>(q, bar)) {
                 steps += 1u;
                 x = q.x;
                 px = q.px;

@@ -132,9 +132,9 @@ __device__ __forceinline__ double radius_fma(const Particle &p) {
 
 // Forward turn in the reference order: sextupole, [octupole], rotate x then
 // y with table[steps] (henon_step, src/henon.cu:493-508, primitives
-// :131-173).  Returns radius_fma of the new state.
+// :131-173).
 template <bool OCT>
-__device__ __forceinline__ double turn_exact_fwd(Particle &p, const Turn &t, double mu) {
+__device__ __forceinline__ void turn_exact_fwd(Particle &p, const Turn &t, double mu) {
     // px += x*x - y*y ; py += (-2*x)*y          (sextupole, :131-143)
     double px = Rn::add(p.px, Rn::sub(p.xx, p.yy));
     double py = Rn::add(p.py, Rn::mul(Rn::mul(-2.0, p.x), p.y));
@@ -151,13 +151,12 @@ __device__ __forceinline__ double turn_exact_fwd(Particle &p, const Turn &t, dou
     const double y = Rn::add(Rn::mul(p.y, t.cy), Rn::mul(py, t.sy));
     py = Rn::add(Rn::mul(-p.y, t.sy), Rn::mul(py, t.cy));
     p = Particle{x, px, y, py, Rn::mul(x, x), Rn::mul(y, y)};
-    return radius_fma(p);
 }
 
 // Reverse turn: rotate x then y backwards with table[steps-1], subtract the
 // octupole, subtract the sextupole (src/henon.cu:510-528).
 template <bool OCT>
-__device__ __forceinline__ double turn_exact_rev(Particle &p, const Turn &t, double mu) {
+__device__ __forceinline__ void turn_exact_rev(Particle &p, const Turn &t, double mu) {
     const double x = Rn::sub(Rn::mul(p.x, t.cx), Rn::mul(p.px, t.sx));
     double px = Rn::add(Rn::mul(p.x, t.sx), Rn::mul(p.px, t.cx));
     const double y = Rn::sub(Rn::mul(p.y, t.cy), Rn::mul(p.py, t.sy));
@@ -173,14 +172,13 @@ __device__ __forceinline__ double turn_exact_rev(Particle &p, const Turn &t, dou
     px = Rn::sub(px, Rn::sub(xx, yy));
     py = Rn::sub(py, Rn::mul(Rn::mul(-2.0, x), y));
     p = Particle{x, px, y, py, xx, yy};
-    return radius_fma(p);
 }
 
-// The same map with fused multiply-adds and x^3-3xy^2 = x(x^2-3y^2): 14 + 3
-// (mu = 0) / 20 + 3 (mu != 0) FP64 instructions per particle-turn, against
-// 19 + 3 / 33 + 3 for the exact turn.
+// The same map with fused multiply-adds and x^3-3xy^2 = x(x^2-3y^2): 14
+// (mu = 0) / 20 (mu != 0) FP64 instructions per particle-turn, against
+// 19 / 33 for the exact turn (the barrier test adds none in the common case).
 template <bool OCT>
-__device__ __forceinline__ double turn_fast_fwd(Particle &p, const Turn &t, double mu) {
+__device__ __forceinline__ void turn_fast_fwd(Particle &p, const Turn &t, double mu) {
     double px = p.px + (p.xx - p.yy);
     double py = fma(-2.0 * p.x, p.y, p.py);
     if (OCT) {
@@ -192,11 +190,10 @@ __device__ __forceinline__ double turn_fast_fwd(Particle &p, const Turn &t, doub
     const double y = fma(p.y, t.cy, py * t.sy);
     py = fma(py, t.cy, -p.y * t.sy);
     p = Particle{x, px, y, py, x * x, y * y};
-    return radius_fma(p);
 }
 
 template <bool OCT>
-__device__ __forceinline__ double turn_fast_rev(Particle &p, const Turn &t, double mu) {
+__device__ __forceinline__ void turn_fast_rev(Particle &p, const Turn &t, double mu) {
     const double x = fma(p.x, t.cx, -p.px * t.sx);
     double px = fma(p.x, t.sx, p.px * t.cx);
     const double y = fma(p.y, t.cy, -p.py * t.sy);
@@ -210,15 +207,18 @@ __device__ __forceinline__ double turn_fast_rev(Particle &p, const Turn &t, doub
     px = px - (xx - yy);
     py = fma(2.0 * x, y, py);
     p = Particle{x, px, y, py, xx, yy};
-    return radius_fma(p);
 }
 
-// One turn; returns radius_fma of the new state for the barrier test below.
+// One turn of the map; the barrier test is separate (inside_after_turn).
 template <int ARITH, bool OCT, bool REV>
-__device__ __forceinline__ double turn(Particle &p, const Turn &t, double mu) {
-    if (ARITH == HM_ARITH_EXACT)
-        return REV ? turn_exact_rev<OCT>(p, t, mu) : turn_exact_fwd<OCT>(p, t, mu);
-    return REV ? turn_fast_rev<OCT>(p, t, mu) : turn_fast_fwd<OCT>(p, t, mu);
+__device__ __forceinline__ void turn(Particle &p, const Turn &t, double mu) {
+    if (ARITH == HM_ARITH_EXACT) {
+        if (REV) turn_exact_rev<OCT>(p, t, mu);
+        else turn_exact_fwd<OCT>(p, t, mu);
+    } else {
+        if (REV) turn_fast_rev<OCT>(p, t, mu);
+        else turn_fast_fwd<OCT>(p, t, mu);
+    }
 }
 
 // ---- reproducible random kicks ---------------------------------------------------
@@ -333,26 +333,73 @@ __device__ __forceinline__ void apply_kick(Particle &p, const KickDirection &d, 
 // radius_fma itself (margin 0).
 constexpr unsigned long long kBarrierMargin = 64ull;
 
+// Before any of that, a test on the coordinates alone, on the integer pipe:
+// if |x|, |px|, |y|, |py| are all below T = sqrt(barrier^2)/2 (1 - 2^-20),
+// every computed sum of their squares (either grouping, with or without
+// FMAs: at most four roundings of non-negative terms, each below T^2) is
+// below 4 T^2 (1 + 2^-50) < barrier^2, so the particle is inside in both
+// arithmetic modes.  The test compares the high words of |c|'s bit
+// patterns with that of T (a smaller high word means a smaller value; NaN
+// and infinities lie above every finite T).  barrier^2 = +inf takes
+// T = sqrt(DBL_MAX)/2 (1 - 2^-20), so that the bound stays finite; a NaN
+// barrier arrives as pattern 0 and disables the test, as does a tiny one.
+// In a stable orbit every coordinate stays far below the barrier, so the
+// common case spends no FP64 instruction on the barrier at all.
 struct Barrier {
     unsigned long long b2;  // pattern of barrier^2 (0 for a NaN barrier)
     unsigned long long lo;  // patterns below lo: inside for certain
     unsigned long long hi;  // exact arithmetic: patterns above hi are outside
+    uint32_t small_hi;      // high word of T: all |c| high words below it: inside
 };
+
+__device__ __forceinline__ uint32_t small_threshold_hi(unsigned long long b2) {
+    const double r2 = fmin(__longlong_as_double(static_cast<long long>(b2)), 1.7976931348623157e308);
+    // Near the subnormal range rounding errors are absolute, not relative:
+    // a barrier^2 below 2^-900 disables the test (above it the margin
+    // r2 2^-19 always exceeds four subnormal rounding errors of 2^-1075).
+    if (!(r2 >= 0x1p-900)) return 0u;
+    const double t = Rn::mul(Rn::mul(__dsqrt_rn(r2), 0.5), 1.0 - 0x1p-20);
+    return static_cast<uint32_t>(__double2hiint(t));
+}
 
 template <int ARITH>
 __device__ __forceinline__ Barrier make_barrier(long long b2bits) {
     const unsigned long long b2 = static_cast<unsigned long long>(b2bits);
-    if (ARITH != HM_ARITH_EXACT) return Barrier{b2, b2, b2};
+    const uint32_t small_hi = small_threshold_hi(b2);
+    if (ARITH != HM_ARITH_EXACT) return Barrier{b2, b2, b2, small_hi};
     const unsigned long long lo = b2 > kBarrierMargin ? b2 - kBarrierMargin : 0ull;
     const unsigned long long hi = b2 < ~0ull - kBarrierMargin ? b2 + kBarrierMargin : ~0ull;
-    return Barrier{b2, lo, hi};
+    return Barrier{b2, lo, hi, small_hi};
 }
 
 __device__ __forceinline__ unsigned long long pattern(double r) {
     return static_cast<unsigned long long>(__double_as_longlong(r));
 }
 
-// Common case: r_fma decides "inside" on its own.
+__device__ __forceinline__ uint32_t abs_hi(double v) {
+    return static_cast<uint32_t>(__double2hiint(v)) & 0x7fffffffu;
+}
+
+// OR of the high words of the four coordinates.  With the sign bit masked
+// off, an OR of high words is at least each of them, so an OR below
+// small_hi passes small_inside for every coordinate it covers: a thread
+// ORs all its particles and compares once (three-input LOP3s, no FP64).
+__device__ __forceinline__ uint32_t hi_or(const Particle &p) {
+    return static_cast<uint32_t>(__double2hiint(p.x)) | static_cast<uint32_t>(__double2hiint(p.px)) |
+           static_cast<uint32_t>(__double2hiint(p.y)) | static_cast<uint32_t>(__double2hiint(p.py));
+}
+
+__device__ __forceinline__ bool small_or(uint32_t ored, const Barrier &b) {
+    return (ored & 0x7fffffffu) < b.small_hi;
+}
+
+// Every coordinate is small (no FP64 instruction).
+__device__ __forceinline__ bool small_inside(const Particle &p, const Barrier &b) {
+    const uint32_t m = max(max(abs_hi(p.x), abs_hi(p.px)), max(abs_hi(p.y), abs_hi(p.py)));
+    return m < b.small_hi;
+}
+
+// Next case: r_fma decides "inside" on its own.
 __device__ __forceinline__ bool surely_inside(double r_fma, const Barrier &b) {
     return pattern(r_fma) < b.lo;
 }
@@ -368,6 +415,14 @@ __device__ __forceinline__ bool settle_inside(double r_fma, const Particle &p, c
 template <int ARITH>
 __device__ __forceinline__ bool inside(double r_fma, const Particle &p, const Barrier &b) {
     return surely_inside(r_fma, b) || settle_inside<ARITH>(r_fma, p, b);
+}
+
+// The whole decision for a particle after a turn: the coordinate test,
+// then the FMA sum, then (exact arithmetic, near the barrier) the
+// reference's sum.
+template <int ARITH>
+__device__ __forceinline__ bool inside_after_turn(const Particle &p, const Barrier &b) {
+    return small_inside(p, b) || inside<ARITH>(radius_fma(p), p, b);
 }
 
 // Jacobian of one turn, row-major, in the reference's expression order

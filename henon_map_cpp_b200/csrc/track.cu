@@ -31,18 +31,19 @@ using dev::Rn;
 using dev::Turn;
 
 // One turn of the K particles of a thread.  The common case costs the map
-// and one integer compare per particle; a warp with a particle near or past
-// the barrier takes the rare path, which settles the test and freezes lost
-// particles (set_to_nan, src/henon.cu:123-129) with steps = the turns they
-// survived.
+// and, per thread, an OR of the coordinates' high words and one integer
+// compare (dev::small_or); a warp with a thread whose coordinates are not
+// all small takes the rare path, which settles the barrier test per
+// particle and freezes lost particles (set_to_nan, src/henon.cu:123-129)
+// with steps = the turns they survived.  A lost particle's registers are
+// set to zero, a fixed point of the map, so that it never trips the OR
+// again.
 template <int ARITH, bool OCT, bool REV, int K, bool KICK>
 __device__ __forceinline__ void turn_all(const TrackChunk &c, const Barrier &bar, double mu,
                                          const Turn &t, uint32_t k, Particle (&p)[K],
                                          const uint32_t (&id)[K], bool (&live)[K],
                                          bool &warp_live) {
-    double r[K];
-    bool check[K];
-    bool any_check = false;
+    uint32_t ored = 0u;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
         // Random kick: before the sextupole going forward (table index
@@ -51,21 +52,19 @@ __device__ __forceinline__ void turn_all(const TrackChunk &c, const Barrier &bar
         if (KICK && !REV)
             dev::apply_kick<false>(p[j], dev::kick_direction(c.kick_seed, id[j], c.turn0 + k),
                                    c.kick_module);
-        r[j] = dev::turn<ARITH, OCT, REV>(p[j], t, mu);
-        if (KICK && REV) {
+        dev::turn<ARITH, OCT, REV>(p[j], t, mu);
+        if (KICK && REV)
             dev::apply_kick<true>(p[j], dev::kick_direction(c.kick_seed, id[j], c.turn0 - 1u - k),
                                   c.kick_module);
-            r[j] = dev::radius_fma(p[j]);
-        }
-        check[j] = live[j] && !dev::surely_inside(r[j], bar);
-        any_check |= check[j];
+        if (!KICK || live[j]) ored |= dev::hi_or(p[j]);
     }
-    if (__any_sync(kFullMask, any_check)) {
+    if (__any_sync(kFullMask, !dev::small_or(ored, bar))) {
         const uint32_t s = REV ? c.turn0 - k : c.turn0 + k;
         bool any_live = false;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            if (check[j] && !dev::settle_inside<ARITH>(r[j], p[j], bar)) {
+            if (live[j] && !dev::small_inside(p[j], bar) &&
+                !dev::inside<ARITH>(dev::radius_fma(p[j]), p[j], bar)) {
                 const uint32_t i = id[j];
                 c.ux[i] = quiet_nan();
                 c.upx[i] = quiet_nan();
@@ -73,6 +72,7 @@ __device__ __forceinline__ void turn_all(const TrackChunk &c, const Barrier &bar
                 c.upy[i] = quiet_nan();
                 c.usteps[i] = s;
                 live[j] = false;
+                p[j] = dev::make_particle(0.0, 0.0, 0.0, 0.0);
             }
             any_live |= live[j];
         }
@@ -180,8 +180,10 @@ __device__ __forceinline__ bool turns_staged(const TrackChunk &c, const Barrier 
 }
 
 // One chunk of turns for the particles of one block (K per thread).
+// At most two particles per thread the kernel fits 64 registers without
+// spills, i.e. 8 blocks of 128 threads per SM; four per thread need more.
 template <int ARITH, bool OCT, bool REV, int K, bool STAGED, bool KICK>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, K <= 2 ? 4 : 1)
 track_chunk_kernel(const TrackChunk c) {
     const uint32_t n_in = c.in_count ? *c.in_count : c.n_user;
     const uint32_t base = blockIdx.x * (blockDim.x * K);
@@ -213,6 +215,8 @@ track_chunk_kernel(const TrackChunk c) {
                 live[j] = !(isnan(x) || isnan(px) || isnan(y) || isnan(py));
             }
         }
+        // Slots without a live particle hold zeros, a fixed point of the map.
+        if (!live[j]) x = px = y = py = 0.0;
         p[j] = dev::make_particle(x, px, y, py);
     }
 

@@ -43,8 +43,8 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     for (uint32_t k = 0; k < a.n_turns; ++k) {
         if (alive) {
-            const double r = dev::turn<ARITH, OCT, false>(p, dev::load_turn(a.table, a.live_step + k), a.mu);
-            if (dev::inside<ARITH>(r, p, bar)) {
+            dev::turn<ARITH, OCT, false>(p, dev::load_turn(a.table, a.live_step + k), a.mu);
+            if (dev::inside_after_turn<ARITH>(p, bar)) {
                 steps += 1u;
                 x = p.x;
                 px = p.px;

@@ -407,14 +407,21 @@ hm_status hm_batch_create(size_t n_sets, const hm_batch_set *sets,
                           hm_batch **out);
 hm_status hm_batch_destroy(hm_batch *b);
 /* Arithmetic, particles per thread (1, 2, 4) and the chunk schedule (first
- * chunk, cap of the doubling length); chosen by the autotuner. */
+ * chunk, cap of the doubling length; default 512 and 4096); chosen by the
+ * autotuner. */
 hm_status hm_batch_configure(hm_batch *b, hm_arith arith, int per_thread,
                              uint32_t chunk0, uint32_t chunk_max);
 /* Splits the sets into `groups` (1..8) groups of about equal work, each
  * tracked by its own chain of chunk launches on its own stream, so that
- * one group's chunk ramp-down overlaps another group's work (default 4).
+ * one group's chunk ramp-down overlaps another group's work (default 8).
  * Results do not depend on it. */
 hm_status hm_batch_set_groups(hm_batch *b, int groups);
+/* Grid of each group's chunk kernel: share x (the group's particles x
+ * turns) / (all sets'), as a fraction of the device's resident blocks, at
+ * most all of them (default 1.5; 0 gives every group the whole device).
+ * Smaller grids running side by side spend less of each launch in its
+ * last, partly empty round of tiles.  Results do not depend on it. */
+hm_status hm_batch_set_grid_share(hm_batch *b, double share);
 hm_status hm_batch_size(const hm_batch *b, uint64_t *n_total,
                         uint32_t *n_chunks);
 /* Initial conditions of all sets, concatenated in set order (host). */

@@ -95,16 +95,39 @@ def test_batch_barriers_at_the_last_bit(gpu, arith):
             np.testing.assert_array_equal(r["steps"], o[4])
 
 
+def test_batch_barrier_scales_match_oracle(gpu):
+    # One set per barrier scale (subnormal square, small, large, overflowing
+    # square, +inf, NaN) in one batch: exact decisions equal the oracle's.
+    from conftest import TUNES, grid
+    from oracle import oracle as O
+
+    barriers = [1e-160, 1e-3, 0.2, 0.5, 3.0, 1e10, 1e200, np.inf, np.nan]
+    x, px, y, py = grid(0.6, 16)
+    n_turns, eps, mu = 300, 16.0, 0.2
+    sets = [dict(omega_x=TUNES[0], omega_y=TUNES[1], epsilon=eps, mu=mu, n_particles=x.size,
+                 n_turns=n_turns, barrier=b) for b in barriers]
+    coords = tuple(np.tile(c, len(sets)) for c in (x, px, y, py))
+    res = sweep.run_sweep(sets, coords, arith=0, chunk0=64, chunk_max=128)
+    tabs = O.tables(n_turns, *TUNES, "sps", epsilon=eps)
+    for s, r in zip(sets, res):
+        o = O.track(x, px, y, py, np.zeros(x.size, np.uint32), tabs, n_turns, mu, s["barrier"])
+        np.testing.assert_array_equal(r["steps"], o[4], err_msg=f"barrier {s['barrier']!r}")
+        for k, w in zip(("x", "px", "y", "py"), o[:4]):
+            assert_bitwise(r[k], w, k)
+
+
 def test_batch_groups_do_not_change_results(gpu):
-    # Sets split into 1..8 concurrently tracked groups: each set still ends
+    # Sets split into 1..8 concurrently tracked groups, with grids from a
+    # single block per group to the whole device: each set still ends
     # exactly as a plain hm_track of it alone.
     sets, coords = sweep.heterogeneous_sets(seed=23, n_sets=11, n_range=(40, 2000),
                                             turn_range=(50, 5000))
     b = C.Batch(sets)
     b.load(*coords)
     outs = []
-    for g in (1, 3, 8):
+    for g, share in ((1, 0.0), (3, 1.5), (8, 1.5), (8, 1e-9), (8, 0.0)):
         b.set_groups(g)
+        b.set_grid_share(share)
         b.configure(C.ARITH_EXACT, 1, 128, 1024)
         b.run(True)
         outs.append([b.get(f) for f in (C.FIELD_X, C.FIELD_PY, C.FIELD_STEPS)])
@@ -119,3 +142,6 @@ def test_batch_groups_do_not_change_results(gpu):
         o += n
     with pytest.raises(C.HMError):
         b.set_groups(9)
+    for bad in (-1.0, float("inf"), float("nan")):
+        with pytest.raises(C.HMError):
+            b.set_grid_share(bad)

@@ -90,6 +90,47 @@ def test_barrier_decided_at_the_last_bit(gpu):
     assert all(v == {True, False} for v in kept.values())
 
 
+# Barriers across scales: a square in the subnormal range (the coordinate
+# test is off), small and large ones (the coordinate test decides most
+# turns), one whose square overflows to +inf, +inf itself and NaN.
+SCALE_BARRIERS = [1e-160, 1e-3, 0.2, 0.5, 1.0, 3.0, 1e10, 1e160, 1e200, np.inf, np.nan]
+
+
+@pytest.mark.parametrize("barrier", SCALE_BARRIERS)
+def test_barrier_scales_match_oracle(gpu, barrier):
+    x, px, y, py = grid(0.6, 32)
+    got, _, _ = run_gpu(x, px, y, py, 400, 16.0, 0.2, barrier=barrier)
+    want = run_oracle(x, px, y, py, 400, 16.0, 0.2, barrier=barrier)
+    np.testing.assert_array_equal(got[4], want[4], err_msg=f"barrier {barrier!r}")
+    for a, w in zip(got[:4], want[:4]):
+        assert_bitwise(a, w, f"barrier {barrier!r}")
+
+
+def test_barrier_at_twice_the_largest_coordinate(gpu):
+    # The coordinate test passes a particle when every |c| is below
+    # T = barrier/2 (1 - 2^-20).  Barriers around twice a particle's
+    # largest coordinate put that threshold on both sides of the
+    # coordinate it reaches; the decisions must stay the oracle's.
+    x, px, y, py = grid(0.5, 8)
+    n_turns, eps, mu = 300, 16.0, 0.2
+    tabs = O.tables(n_turns, *TUNES, "sps", epsilon=eps)
+    st = (x, px, y, py, np.zeros(x.size, np.uint32))
+    cmax = np.zeros(x.size)
+    with np.errstate(all="ignore"):
+        for _ in range(n_turns):
+            st = O.track(*st, tabs, 1, mu, 1e200)
+            cmax = np.fmax(cmax, np.max(np.abs(np.stack(st[:4])), axis=0))
+    ok = np.flatnonzero(np.isfinite(cmax) & (cmax > 0.05) & (cmax < 5.0))
+    for i in ok[np.linspace(0, ok.size - 1, 4).astype(int)]:
+        for f in (1 - 2.0**-18, 1 - 2.0**-21, 1.0, 1 + 2.0**-21, 1 + 2.0**-18):
+            b = float(2.0 * cmax[i] * f)
+            got, _, _ = run_gpu(x, px, y, py, n_turns, eps, mu, barrier=b)
+            want = run_oracle(x, px, y, py, n_turns, eps, mu, barrier=b)
+            np.testing.assert_array_equal(got[4], want[4], err_msg=f"barrier {b!r}")
+            for a, w in zip(got[:4], want[:4]):
+                assert_bitwise(a, w, f"barrier {b!r}")
+
+
 def test_split_calls_equal_one_call(gpu):
     x, px, y, py = grid(0.6, 32)
     one, _, _ = run_gpu(x, px, y, py, 3000, 16.0, 0.2)
