@@ -181,6 +181,7 @@ def reference_cpu_sample(turns: int, side: int, target_s: float = 20.0):
         sel = sel.ravel()
         sx, spx, sy, spy = (np.ascontiguousarray(a[sel]) for a in (x, px, y, py))
         n = sx.size
+        results = {}
         t0 = time.perf_counter()
         for eps in EPSILONS:
             if kind == "reference":
@@ -191,18 +192,30 @@ def reference_cpu_sample(turns: int, side: int, target_s: float = 20.0):
                 if kind == "reference":
                     p = R.particles_4d(sx, spx, sy, spy)
                     tr.track(p, turns, mu, BARRIER)
+                    results[(eps, mu)] = p
                 else:
-                    O.track(sx, spx, sy, spy, np.zeros(n, np.uint32), tabs, turns, mu, BARRIER)
+                    results[(eps, mu)] = O.track(sx, spx, sy, spy, np.zeros(n, np.uint32), tabs,
+                                                 turns, mu, BARRIER)
         dt = time.perf_counter() - t0
         if dt >= target_s / 4 or stride <= 4:
             break
         stride //= 2
     nominal = n * turns * len(EPSILONS) * len(MUS)
     cores = os.cpu_count() if kind == "reference" else O.max_threads()
+    # Final states of the sample (outside the timed region), for the parity
+    # check of the GPU's exact arithmetic against this CPU path.
+    states = {}
+    for key, r in results.items():
+        if kind == "reference":
+            states[key] = tuple(np.asarray(a) for a in (r.get_x(), r.get_px(), r.get_y(),
+                                                        r.get_py(), r.get_steps()))
+        else:
+            states[key] = tuple(np.asarray(a) for a in r[:5])
     return {"value": nominal / dt, "unit": UNIT, "cores": cores, "kind": kind,
             "sample": f"every {stride}th grid point per axis ({n} particles) x {turns} turns x "
                       f"6 (eps, mu) scans = {nominal:.3g} nominal particle-turns in {dt:.2f} s "
-                      f"(table setup included)"}
+                      f"(table setup included)",
+            "_sel": np.flatnonzero(sel), "_states": states}
 
 
 # ---- supplementary measurements (one GPU) ---------------------------------------------
@@ -504,6 +517,21 @@ def run_ours(args):
                 flops += s * FLOPS_PER_TURN[mu != 0.0]
         return executed, flops
 
+    def final_states(mode):
+        """One untimed step; each scan's final x, px, y, py, steps (host)."""
+        out = {}
+        for eps in EPSILONS:
+            tab = trackers[eps].device_tables()
+            for mu in MUS:
+                for w, d in zip(work, dev0):
+                    w.copy_(d)
+                steps.zero_()
+                C.call("hm_track_device", *[w.data_ptr() for w in work], steps.data_ptr(), n,
+                       tab, args.turns, 0, args.turns, mu, BARRIER, 0, mode, ws.data_ptr(), sptr)
+                out[(eps, mu)] = tuple(w.cpu().numpy() for w in work) + (
+                    steps.cpu().numpy().view(np.uint32),)
+        return out
+
     def barrier():
         if dist is not None:
             dist.barrier()
@@ -639,6 +667,46 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu_sample(args.turns, args.side)
 
+    # Parity of this run's results (one untimed step per arithmetic): the
+    # exact arithmetic against the reference's CPU path on the CPU leg's
+    # sample, bit for bit; the fast arithmetic against the exact on the
+    # whole grid (survival turns).
+    parity = None
+    if world == 1:
+        exact_states = final_states(C.ARITH_EXACT)
+        fast_states = final_states(C.ARITH_FAST)
+        pts = same_steps = same_survival = 0
+        for key, (_, _, _, _, se) in exact_states.items():
+            sf = fast_states[key][4]
+            pts += se.size
+            same_steps += int(np.count_nonzero(se == sf))
+            same_survival += int(np.count_nonzero((se == args.turns) == (sf == args.turns)))
+        parity = {"fast_vs_exact": {"grid_points": pts,
+                                    "survival_turns_equal": same_steps / pts,
+                                    "survival_equal": same_survival / pts}}
+        del fast_states
+        if cpu is not None:
+            sel = cpu["_sel"]
+            n_cmp = steps_eq = coords_eq = 0
+            for key, ref in cpu["_states"].items():
+                got = exact_states[key]
+                n_cmp += sel.size
+                steps_eq += int(np.count_nonzero(got[4][sel] == ref[4].astype(np.uint32)))
+                same = np.ones(sel.size, bool)
+                for k in range(4):
+                    a = got[k][sel].copy()
+                    b = np.array(ref[k], dtype=np.float64)
+                    a[np.isnan(a)] = np.nan  # one NaN pattern on both sides
+                    b[np.isnan(b)] = np.nan
+                    same &= a.view(np.uint64) == b.view(np.uint64)
+                coords_eq += int(np.count_nonzero(same))
+            parity["exact_vs_cpu_baseline"] = {
+                "kind": cpu["kind"], "particles": n_cmp,
+                "survival_turns_equal": steps_eq / n_cmp, "coordinates_bit_equal": coords_eq / n_cmp}
+        del exact_states
+    if cpu is not None:
+        cpu = {k: v for k, v in cpu.items() if not k.startswith("_")}
+
     extras = {}
     if world == 1 and not args.no_extras:
         extras["batched"] = bench_batched(C, arith)
@@ -675,6 +743,7 @@ def run_ours(args):
             "clocks": clock_summary,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "parity": parity,
             **extras,
         }
         print(json.dumps(line), flush=True)
