@@ -29,15 +29,31 @@ namespace {
 
 using dev::Rn;
 
-template <bool OCT, bool DO_M, bool DO_V, bool DO_T>
-__global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
+// SPLIT: every particle is followed by two warps.  Both track it (the
+// same operations, so the same orbit); the even warp of a pair also carries
+// the tangent matrix, MEGNO and the MEGNO-Birkhoff windows, the odd one the
+// tangent vector, the Lyapunov windows and the tunes.  Each thread then
+// holds about half of a particle's window accumulators, so the same shared
+// memory holds twice the threads: the loop is a long chain of dependent
+// FP64 operations, and more warps per SM hide its latency.
+template <bool OCT, bool DO_M, bool DO_V, bool DO_T, bool SPLIT>
+__global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const FusedArgs a) {
     extern __shared__ double smem[];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    // Role of this warp: with SPLIT, even warps do the matrix work and odd
+    // warps the vector and tune work; without it, every warp does all.
+    const bool role_m = !SPLIT || (warp & 1u) == 0u;
+    const bool role_v = !SPLIT || (warp & 1u) == 1u;
+    const bool do_m = DO_M && role_m, do_v = DO_V && role_v, do_t = DO_T && role_v;
+    // Threads (per role) of a block, and this thread's index among them.
+    const int T = SPLIT ? int(blockDim.x) / 2 : int(blockDim.x);
+    const int tid = SPLIT ? int((warp >> 1) * 32u + lane) : int(threadIdx.x);
+    const uint32_t i = blockIdx.x * uint32_t(T) + uint32_t(tid);
     const bool in_range = i < a.n;
     const uint32_t ii = in_range ? i : 0;
     // Per-thread window accumulators in shared memory, laid out [slot][thread]
-    // so that a warp touches 32 consecutive doubles.
-    const int T = blockDim.x;
+    // so that a warp touches 32 consecutive doubles.  With SPLIT the matrix
+    // role's slots come first, then the vector role's, each T threads wide.
     double *mb_l2 = smem;                                  // [n_mb][T]
     double *ly_raw = mb_l2 + size_t(a.n_mb) * T;           // [n_ly][T]
     double *ly_b = ly_raw + size_t(a.n_ly) * T;            // [n_ly][T]
@@ -45,7 +61,6 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     double *t1y = t1x + size_t(a.n_tu) * T;
     double *t2x = t1y + size_t(a.n_tu) * T;
     double *t2y = t2x + size_t(a.n_tu) * T;
-    const int tid = threadIdx.x;
     const size_t n = a.n;
 
     // ---- load state ---------------------------------------------------------
@@ -54,7 +69,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     bool alive = in_range && !dev::is_lost(x, px, y, py);
     double M[16];
     double old_norm = 0.0, m_l1 = 0.0, m_l2 = 0.0, m_l3 = 0.0, b_l1 = 0.0;
-    if (DO_M) {
+    if (do_m) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) M[k] = a.M[size_t(ii) * 16 + k];
         old_norm = dev::norm_exact<16>(M);
@@ -67,7 +82,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
         for (int w = 0; w < a.n_mb; ++w) mb_l2[w * T + tid] = a.mb_l2[w * n + ii];
     }
     double v[4] = {0.0, 0.0, 0.0, 0.0};
-    if (DO_V) {
+    if (do_v) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) v[k] = a.V[size_t(ii) * 4 + k];
         for (int w = 0; w < a.n_ly; ++w) {
@@ -76,7 +91,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
         }
     }
     double store_x = 0.0, store_y = 0.0;
-    if (DO_T) {
+    if (do_t) {
         store_x = a.store_x[ii];
         store_y = a.store_y[ii];
         for (int w = 0; w < a.n_tu; ++w) {
@@ -94,7 +109,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     for (; k < a.n_turns && warp_live; ++k) {
         double df[16];
         // ---- Jacobian of the turn, at the point before it (option) ------------
-        if ((DO_M || DO_V) && a.df_before) {
+        if ((do_m || do_v) && a.df_before) {
             const dev::Turn td = dev::load_turn(a.table, a.live_step + k);
             dev::tangent_matrix_exact(x, y, td, mu, df);
         }
@@ -115,11 +130,11 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
             }
         }
         // ---- tangent matrix at the new point, table[global_steps] -------------
-        if ((DO_M || DO_V) && !a.df_before) {
+        if ((do_m || do_v) && !a.df_before) {
             const dev::Turn td = dev::load_turn(a.table, a.global_step + k + 1u);
             dev::tangent_matrix_exact(x, y, td, mu, df);
         }
-        if (DO_M) {
+        if (do_m) {
             double out[16];
             dev::matmul4_exact(df, M, out);
 #pragma unroll
@@ -147,7 +162,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
             }
             old_norm = new_norm;
         }
-        if (DO_V) {
+        if (do_v) {
             double t4[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
@@ -172,7 +187,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) v[q] = Rn::div(t4[q], nv);
         }
-        if (DO_T) {
+        if (do_t) {
             const double ax = atan2(px, x), ay = atan2(py, y);
             double dx = Rn::sub(ax, store_x), dy = Rn::sub(ay, store_y);
             const double two_pi = 2 * M_PI;
@@ -203,18 +218,18 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     if (k < a.n_turns) {
         const double nan = dev::quiet_nan();
         const uint64_t left = a.n_turns - k;  // turns skipped
-        if (DO_M && a.megno_l1)
+        if (do_m && a.megno_l1)
             for (int j = 0; j < a.n_snap; ++j) {
                 const uint64_t s = a.snap_turns[j];
                 if (s >= a.megno_idx + k && s < a.megno_idx + a.n_turns && in_range)
                     a.snap[size_t(j) * n + ii] = nan;
             }
-        if (DO_M && a.mb_l1) {
+        if (do_m && a.mb_l1) {
             const uint64_t idx = a.mb_idx + k;
             for (int w = 0; w < a.n_mb; ++w)
                 if (idx <= a.mb_T[w]) mb_l2[w * T + tid] = nan;
         }
-        if (DO_V) {
+        if (do_v) {
             const uint64_t idx = a.ly_idx + k;
             for (int w = 0; w < a.n_ly; ++w)
                 if (idx < a.ly_len[w]) {
@@ -222,7 +237,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
                     ly_b[w * T + tid] = nan;
                 }
         }
-        if (DO_T) {
+        if (do_t) {
             const uint64_t first = a.tu_idx + k, last = a.tu_idx + k + left - 1;
             for (int w = 0; w < a.n_tu; ++w) {
                 const uint64_t len = a.tu_T[w];
@@ -240,13 +255,15 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     }
 
     if (!in_range) return;
-    // ---- store state --------------------------------------------------------
-    a.x[i] = x;
-    a.px[i] = px;
-    a.y[i] = y;
-    a.py[i] = py;
-    a.steps[i] = steps;
-    if (DO_M) {
+    // ---- store state (both roles hold the same orbit; one writes it) ---------
+    if (role_m) {
+        a.x[i] = x;
+        a.px[i] = px;
+        a.y[i] = y;
+        a.py[i] = py;
+        a.steps[i] = steps;
+    }
+    if (do_m) {
 #pragma unroll
         for (int q = 0; q < 16; ++q) a.M[size_t(i) * 16 + q] = M[q];
         if (a.megno_l1) {
@@ -257,7 +274,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
         if (a.mb_l1) a.mb_l1[i] = b_l1;
         for (int w = 0; w < a.n_mb; ++w) a.mb_l2[w * n + i] = mb_l2[w * T + tid];
     }
-    if (DO_V) {
+    if (do_v) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) a.V[size_t(i) * 4 + q] = v[q];
         for (int w = 0; w < a.n_ly; ++w) {
@@ -265,7 +282,7 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
             a.ly_b[w * n + i] = ly_b[w * T + tid];
         }
     }
-    if (DO_T) {
+    if (do_t) {
         a.store_x[i] = store_x;
         a.store_y[i] = store_y;
         for (int w = 0; w < a.n_tu; ++w) {
@@ -277,18 +294,22 @@ __global__ void __launch_bounds__(128) indicators_kernel(const FusedArgs a) {
     }
 }
 
+// The matrix and the vector/tune work are split over two warps per particle
+// when both are requested (64 particles per block of 128 threads).
 template <bool OCT, bool DO_M, bool DO_V, bool DO_T>
 cudaError_t launch4(const FusedArgs &a, cudaStream_t s) {
     constexpr int threads = 128;
+    constexpr bool split = DO_M && (DO_V || DO_T);
+    constexpr int per_block = split ? threads / 2 : threads;  // particles
     const size_t slots = size_t(a.n_mb) + 2 * size_t(a.n_ly) + 4 * size_t(a.n_tu);
-    const size_t smem = slots * threads * sizeof(double);
-    auto k = indicators_kernel<OCT, DO_M, DO_V, DO_T>;
+    const size_t smem = slots * per_block * sizeof(double);
+    auto k = indicators_kernel<OCT, DO_M, DO_V, DO_T, split>;
     if (smem > 48 * 1024) {
         const cudaError_t e =
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    const unsigned blocks = unsigned((a.n + threads - 1) / threads);
+    const unsigned blocks = unsigned((a.n + per_block - 1) / per_block);
     k<<<blocks, threads, smem, s>>>(a);
     return cudaGetLastError();
 }
