@@ -126,6 +126,46 @@ def test_fused_equals_per_call_loop(gpu, eps, mu):
     assert np.isnan(got["megno"][:32]).all()
 
 
+@pytest.mark.parametrize("use", ["MVT", "MV", "MT", "VT", "M", "V", "T"])
+def test_fused_subsets_equal_per_call_loop(gpu, use):
+    # Every combination of constructs runs its own kernel variant (with the
+    # matrix and the vector or tune work split over two warps per particle
+    # when both are present); each must give the per-call loop's values.
+    x, px, y, py = grid(0.55, 12)
+    n_turns = 400
+    ref = per_call_loop(x, px, y, py, n_turns, 32.0, 0.2)
+    n = len(x)
+    t = C.Tracker(n_turns + 1, TUNES[0], TUNES[1], "sps", NAN, 32.0, 0)
+    p = C.Particles(x, px, y, py)
+    kw = {}
+    if "M" in use:
+        M, M_old = C.Matrices(n), C.Matrices(n)
+        mg, mb = C.Megno(n), C.MegnoBirkhoff(n, MB_W)
+        kw.update(matrix=M, matrix_old=M_old, megno=mg, megno_birkhoff=mb)
+    if "V" in use:
+        v = C.Vectors(np.tile(np.asarray((1.0, 0.0, 0.0, 0.0)), (n, 1)))
+        ly = C.Lyapunov(n, LY_W)
+        kw.update(vectors=v, lyapunov=ly)
+    if "T" in use:
+        tu = C.TuneBirkhoff(n, TU_W)
+        tu.first_add(p)
+        kw.update(tune=tu)
+    for part in (150, 250):
+        C.track_indicators(t, p, part, 0.2, 10.0, **kw)
+    for a, b in zip(p.state(), ref["state"]):
+        assert_bitwise(a, b) if a.dtype == np.float64 else np.testing.assert_array_equal(a, b)
+    if "M" in use:
+        for k, got in (("M", M.get()), ("M_old", M_old.get()), ("megno", mg.get()),
+                       ("mb", mb.get())):
+            assert_bitwise(got, ref[k], f"{use}:{k}")
+    if "V" in use:
+        for k, got in (("v", v.get()), ("ly_raw", ly.get(False)), ("ly_b", ly.get(True))):
+            assert_bitwise(got, ref[k], f"{use}:{k}")
+    if "T" in use:
+        for j, k in enumerate(("t1x", "t1y", "t2x", "t2y")):
+            assert_bitwise(tu.get(j), ref[k], f"{use}:{k}")
+
+
 def test_fused_megno_samples(gpu):
     x, px, y, py = grid(0.5, 10)
     samples = [1, 7, 64, 200, 399, 400, 401, 10_000]
