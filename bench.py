@@ -248,7 +248,7 @@ def bench_batched(C, arith):
     t0 = time.perf_counter()
     b.run(True)
     t_one_group = time.perf_counter() - t0
-    b.set_groups(8)
+    b.set_groups(16)
     b.set_grid_share(1.5)
     # plain: one chunked tracking call per set on device arrays
     t_plain, equal, o = 0.0, True, 0

@@ -631,7 +631,7 @@ class Batch(_Handle):
              int(chunk_max))
 
     def set_groups(self, groups: int) -> None:
-        """Number of concurrently tracked groups of sets (1..8)."""
+        """Number of concurrently tracked groups of sets (1..16)."""
         call("hm_batch_set_groups", self.h, int(groups))
 
     def set_grid_share(self, share: float) -> None:

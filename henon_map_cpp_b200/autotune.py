@@ -39,7 +39,7 @@ def _current_shape() -> dict:
     shape = dict(zip(("threads", "per_thread", "chunk0", "chunk_max"), C.get_track_config()))
     shape["stage_turns"] = C.get_track_staging()
     return shape
-BATCH_SPACE = {"groups": (8, 4, 2, 1), "grid_share": (1.5, 1.0, 2.0, 0.0),
+BATCH_SPACE = {"groups": (16, 8, 4, 1), "grid_share": (1.5, 1.0, 2.0, 0.0),
                "per_thread": (1, 2, 4), "chunk0": (256, 512, 1024),
                "chunk_max": (4096, 8192, 16384)}
 

@@ -105,7 +105,7 @@ struct hm_batch {
 
 namespace {
 
-constexpr int kMaxGroups = 8;
+constexpr int kMaxGroups = 16;
 
 // Enqueues the whole batch on b->stream: reset from the initial
 // conditions, collect, then one chain of plans and chunks per group,

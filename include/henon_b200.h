@@ -411,10 +411,10 @@ hm_status hm_batch_destroy(hm_batch *b);
  * autotuner. */
 hm_status hm_batch_configure(hm_batch *b, hm_arith arith, int per_thread,
                              uint32_t chunk0, uint32_t chunk_max);
-/* Splits the sets into `groups` (1..8) groups of about equal work, each
+/* Splits the sets into `groups` (1..16) groups of about equal work, each
  * tracked by its own chain of chunk launches on its own stream, so that
- * one group's chunk ramp-down overlaps another group's work (default 8).
- * Results do not depend on it. */
+ * one group's chunk ramp-down overlaps another group's work (default 16,
+ * at most the number of sets).  Results do not depend on it. */
 hm_status hm_batch_set_groups(hm_batch *b, int groups);
 /* Grid of each group's chunk kernel: share x (the group's particles x
  * turns) / (all sets'), as a fraction of the device's resident blocks, at

@@ -117,7 +117,7 @@ def test_batch_barrier_scales_match_oracle(gpu):
 
 
 def test_batch_groups_do_not_change_results(gpu):
-    # Sets split into 1..8 concurrently tracked groups, with grids from a
+    # Sets split into 1..16 concurrently tracked groups, with grids from a
     # single block per group to the whole device: each set still ends
     # exactly as a plain hm_track of it alone.
     sets, coords = sweep.heterogeneous_sets(seed=23, n_sets=11, n_range=(40, 2000),
@@ -125,7 +125,7 @@ def test_batch_groups_do_not_change_results(gpu):
     b = C.Batch(sets)
     b.load(*coords)
     outs = []
-    for g, share in ((1, 0.0), (3, 1.5), (8, 1.5), (8, 1e-9), (8, 0.0)):
+    for g, share in ((1, 0.0), (3, 1.5), (8, 1.5), (16, 1e-9), (11, 0.0)):
         b.set_groups(g)
         b.set_grid_share(share)
         b.configure(C.ARITH_EXACT, 1, 128, 1024)
@@ -141,7 +141,7 @@ def test_batch_groups_do_not_change_results(gpu):
         np.testing.assert_array_equal(outs[0][2][o:o + n], want[4])
         o += n
     with pytest.raises(C.HMError):
-        b.set_groups(9)
+        b.set_groups(17)
     for bad in (-1.0, float("inf"), float("nan")):
         with pytest.raises(C.HMError):
             b.set_grid_share(bad)
