@@ -131,6 +131,35 @@ def test_barrier_at_twice_the_largest_coordinate(gpu):
                 assert_bitwise(a, w, f"barrier {b!r}")
 
 
+@pytest.mark.parametrize("eps,mu", [(64.0, 0.2), (1.0, 0.0)])
+def test_million_turns_on_a_grid_subsample_match_the_reference_cpu(gpu, eps, mu):
+    # The dynamic-aperture scan at its long horizon: every 64th point per
+    # axis of the 1024x1024 grid on [0, 0.6]^2, 10^6 turns.  Survival turns
+    # and coordinates bit for bit against the reference's own CPU tracker
+    # (the C oracle where the reference build is absent).
+    v = np.linspace(0.0, 0.6, 1024)
+    xx, yy = np.meshgrid(v, v)
+    x = np.ascontiguousarray(xx[::64, ::64].ravel())
+    y = np.ascontiguousarray(yy[::64, ::64].ravel())
+    px, py = np.zeros_like(x), np.zeros_like(y)
+    n_turns = 10**6
+    got, _, _ = run_gpu(x, px, y, py, n_turns, eps, mu)
+    R = O.reference_module("fmad_off")
+    if R is not None:
+        t = R.henon_tracker(n_turns, TUNES[0], TUNES[1], "sps", NAN, eps, 0)
+        p = R.particles_4d(x, px, y, py)
+        t.track(p, n_turns, mu, 10.0)
+        want = tuple(np.asarray(a) for a in (p.get_x(), p.get_px(), p.get_y(), p.get_py(),
+                                              p.get_steps()))
+    else:
+        want = run_oracle(x, px, y, py, n_turns, eps, mu)
+    np.testing.assert_array_equal(got[4], np.asarray(want[4], np.uint32))
+    for a, w, name in zip(got[:4], want[:4], ("x", "px", "y", "py")):
+        assert_bitwise(a, w, name)
+    survivors = int((got[4] == n_turns).sum())
+    assert 0 < survivors < x.size  # both stable and lost particles
+
+
 def test_split_calls_equal_one_call(gpu):
     x, px, y, py = grid(0.6, 32)
     one, _, _ = run_gpu(x, px, y, py, 3000, 16.0, 0.2)
