@@ -131,6 +131,33 @@ def test_barrier_at_twice_the_largest_coordinate(gpu):
                 assert_bitwise(a, w, f"barrier {b!r}")
 
 
+def test_unmodulated_scan_at_full_size_matches_the_reference_cpu(gpu):
+    # 10^4 particles on the 100x100 grid of [0, 0.5]^2 (px = py = 0),
+    # tunes (0.168, 0.201) without modulation (epsilon = 0), 10^4 turns,
+    # barrier 10: bit for bit against the reference's CPU tracker (the C
+    # oracle where the reference build is absent); the reference leaves
+    # 8075 of the 10^4 particles alive.
+    v = np.linspace(0.0, 0.5, 100)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    px, py = np.zeros_like(x), np.zeros_like(y)
+    n_turns = 10**4
+    got, _, _ = run_gpu(x, px, y, py, n_turns, 0.0, 0.0)
+    R = O.reference_module("fmad_off")
+    if R is not None:
+        t = R.henon_tracker(n_turns, TUNES[0], TUNES[1], "sps", NAN, 0.0, 0)
+        p = R.particles_4d(x, px, y, py)
+        t.track(p, n_turns, 0.0, 10.0)
+        want = tuple(np.asarray(a) for a in (p.get_x(), p.get_px(), p.get_y(), p.get_py(),
+                                              p.get_steps()))
+    else:
+        want = run_oracle(x, px, y, py, n_turns, 0.0, 0.0)
+    np.testing.assert_array_equal(got[4], np.asarray(want[4], np.uint32))
+    for a, w, name in zip(got[:4], want[:4], ("x", "px", "y", "py")):
+        assert_bitwise(a, w, name)
+    assert int((got[4] == n_turns).sum()) == 8075
+
+
 @pytest.mark.parametrize("eps,mu", [(64.0, 0.2), (1.0, 0.0)])
 def test_million_turns_on_a_grid_subsample_match_the_reference_cpu(gpu, eps, mu):
     # The dynamic-aperture scan at its long horizon: every 64th point per
