@@ -68,7 +68,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched / adjoint / indicator measurements")
-    ap.add_argument("--only", choices=["batched", "adjoint", "indicators", "tunes"], default=None,
+    ap.add_argument("--only", choices=["batched", "adjoint", "indicators", "tunes", "constructs",
+                                       "kicks", "ghosts"], default=None,
                     help="run one supplementary measurement alone and print its JSON")
     ap.add_argument("--extra-side", type=int, default=None,
                     help="grid side of --only indicators / tunes (default 512 / 128)")
@@ -377,6 +378,136 @@ def bench_indicators(C, turns=100_000, side=512):
             "timing": "wall clock around one synchronous call (4096-turn launches)"}
 
 
+def bench_constructs(C, turns=1000, side=256):
+    """The reference's per-turn construct loop (tests/test_new_standard.ipynb:
+    one call per construct and turn, 7 launches a turn) against the fused
+    call, on the same 256x256 grid on [0, 0.4]^2 (eps 32, mu 0), MEGNO,
+    Birkhoff-MEGNO, Lyapunov with tangent vectors and Birkhoff tunes at the
+    windows 100, 300, 1000."""
+    import torch
+
+    v = np.linspace(0.0, 0.4, side)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    z = np.zeros_like(x)
+    n = x.size
+    T = [100, 300, 1000]
+
+    def setup():
+        tr = C.Tracker(turns + 1, 0.168, 0.201, "sps", float("nan"), 32.0, 0)
+        p = C.Particles(x, z, y, z)
+        o = dict(matrix=C.Matrices(n), matrix_old=C.Matrices(n), megno=C.Megno(n),
+                 megno_birkhoff=C.MegnoBirkhoff(n, T),
+                 vectors=C.Vectors(np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))),
+                 lyapunov=C.Lyapunov(n, T), tune=C.TuneBirkhoff(n, T))
+        o["tune"].first_add(p)
+        return tr, p, o
+
+    tr, p, o = setup()
+    J = C.Matrices(n)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(turns):
+        o["matrix_old"].explicit_copy(o["matrix"])
+        tr.track(p, 1, 0.0, 10.0)
+        o["matrix"].structured_multiply(tr, p, 0.0)
+        o["megno"].add(o["matrix"], o["matrix_old"])
+        o["megno_birkhoff"].add(o["matrix"], o["matrix_old"])
+        J.set_with_tracker(tr, p, 0.0)
+        o["vectors"].multiply(J)
+        o["lyapunov"].add(o["vectors"])
+        o["vectors"].normalize()
+        o["tune"].add(p)
+    torch.cuda.synchronize()
+    per_call_s = time.perf_counter() - t0
+    per_call_megno = o["megno"].get()
+
+    tr, p, o = setup()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    C.track_indicators(tr, p, turns, 0.0, 10.0, **o)
+    torch.cuda.synchronize()
+    fused_s = time.perf_counter() - t0
+    same = bool(np.array_equal(o["megno"].get(), per_call_megno, equal_nan=True))
+    return {"workload": f"{side}x{side} grid on [0,0.4]^2, eps 32, mu 0, {turns} turns, MEGNO + "
+                        "Birkhoff-MEGNO + Lyapunov + Birkhoff tunes at windows 100/300/1000",
+            "per_call_s": per_call_s, "fused_s": fused_s, "speedup": per_call_s / fused_s,
+            "fused_particle_turns_per_s": n * turns / fused_s,
+            "per_call_particle_turns_per_s": n * turns / per_call_s,
+            "megno_bit_equal": same,
+            "timing": "wall clock; the per-call loop issues one call per construct and turn"}
+
+
+def bench_kicks(C, turns=10_000, side=512):
+    """Tracking with reproducible random kicks (kick_module 1e-7 every turn,
+    Philox keyed by seed, particle and turn) against the same tracking
+    without kicks: 512x512 grid on [0, 0.5]^2, eps 16, mu 0.2."""
+    import torch
+
+    v = np.linspace(0.0, 0.5, side)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    z = np.zeros_like(x)
+    n = x.size
+    tr = C.Tracker(turns, 0.168, 0.201, "sps", float("nan"), 16.0, 0)
+
+    def run(kick):
+        p = C.Particles(x, z, y, z)
+        p.kick_seed = 12345
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tr.track(p, turns, 0.2, 10.0, kick)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, p
+
+    run(1e-7)
+    plain_s, _ = run(float("nan"))
+    kicked_s, p = run(1e-7)
+    _, p2 = run(1e-7)
+    return {"workload": f"{side}x{side} grid on [0,0.5]^2, eps 16, mu 0.2, {turns} turns, "
+                        "kick_module 1e-7",
+            "kicked_s": kicked_s, "plain_s": plain_s,
+            "kicked_particle_turns_per_s": n * turns / kicked_s,
+            "kicked_over_plain_time": kicked_s / plain_s,
+            "reproducible": bool(np.array_equal(p.get(C.FIELD_X), p2.get(C.FIELD_X),
+                                                equal_nan=True)),
+            "timing": "wall clock around one hm_track call"}
+
+
+def bench_ghosts(C, turns=1000, side=256, every=10):
+    """The displacement (ghost) Lyapunov loop of tests/test_new_standard.ipynb
+    through the drop-in facade: 256x256 base particles on [0, 0.5]^2 with x
+    and y ghosts at 1e-10, tracked `every` turns at a time, displacement read
+    and ghosts renormalised after each step (eps 64, mu 0)."""
+    import torch
+
+    import henon_map_cpp_b200 as hm
+
+    v = np.linspace(0.0, 0.5, side)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    z = np.zeros_like(x)
+    p = hm.particles(x, z, y, z)
+    p.add_ghost(1e-10, "x")
+    p.add_ghost(1e-10, "y")
+    t = hm.henon_tracker(turns + every, 0.168, 0.201, "sps", np.nan, 64.0, 0)
+    lyap = np.zeros(2 * x.size)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(turns // every):
+        t.track(p, every, 0.0)
+        lyap += np.log(np.asarray(p.get_displacement_module()).ravel() / 1e-10)
+        p.renormalize(1e-10)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    n_all = 3 * x.size
+    return {"workload": f"{side}x{side} base particles + x and y ghosts at 1e-10, eps 64, mu 0, "
+                        f"{turns} turns, renormalised every {every}",
+            "seconds": dt, "particle_turns_per_s": n_all * turns / dt,
+            "steps_per_s": (turns // every) / dt,
+            "timing": "wall clock; each step is track + displacement read + renormalize"}
+
+
 # ---- reference arm ---------------------------------------------------------------
 
 def bench_tunes(C, turns=10_000, side=128):
@@ -430,7 +561,10 @@ def run_only(args):
         kw["turns"] = args.extra_turns
     fn = {"batched": lambda: bench_batched(C, arith), "adjoint": lambda: bench_adjoint(C),
           "indicators": lambda: bench_indicators(C, **kw),
-          "tunes": lambda: bench_tunes(C, **kw)}[args.only]
+          "tunes": lambda: bench_tunes(C, **kw),
+          "constructs": lambda: bench_constructs(C, **kw),
+          "kicks": lambda: bench_kicks(C, **kw),
+          "ghosts": lambda: bench_ghosts(C, **kw)}[args.only]
     print(json.dumps({"only": args.only, **fn()}), flush=True)
 
 
@@ -713,6 +847,9 @@ def run_ours(args):
         extras["adjoint"] = bench_adjoint(C)
         extras["indicators"] = bench_indicators(C)
         extras["tunes"] = bench_tunes(C)
+        extras["constructs"] = bench_constructs(C)
+        extras["kicks"] = bench_kicks(C)
+        extras["ghosts"] = bench_ghosts(C)
 
     if rank == 0:
         peak_unit = "TFLOP/s"
