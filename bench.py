@@ -103,6 +103,16 @@ def grid_slice(side: int, rank: int, world: int):
 
 # ---- clocks --------------------------------------------------------------------
 
+def smi_id(local: int) -> str:
+    """nvidia-smi's name for CUDA device `local`: nvidia-smi numbers all of
+    the machine's GPUs, CUDA only those in CUDA_VISIBLE_DEVICES (given as
+    indices or UUIDs), so the visible list maps one onto the other."""
+    vis = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    if local < len(vis):
+        return vis[local]
+    return str(local)
+
+
 class ClockSampler:
     """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
 
@@ -111,7 +121,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
-        self.dev = device_index
+        self.dev = smi_id(device_index)
         self.proc = None
         self.lines: list[str] = []
         self.thread = None
