@@ -8,6 +8,13 @@ replayed CUDA graph of persistent chunk launches.
 
     sets = heterogeneous_sets(seed=20261203)           # or sweep_sets(...)
     result = run_sweep(sets, points)                   # steps per set
+
+The reference's job list (configs/all_jobs.txt, one "omega_x omega_y
+epsilon mu max_radius" line per job) runs as one batch too, writing one
+result file per job as its run_sim.py does:
+
+    python -m henon_map_cpp_b200.sweep --jobs configs/all_jobs.txt \
+        --num_points 100 --num_iterations 100000 --out results/
 """
 from __future__ import annotations
 
@@ -60,7 +67,7 @@ def sweep_sets(omega_pairs, epsilons, mus, n_particles: int, n_turns: int,
 
 
 def run_sweep(sets, coords, arith: int = C.ARITH_EXACT, per_thread: int = 1,
-              chunk0: int = 512, chunk_max: int = 16384, use_graph: bool = True):
+              chunk0: int = 512, chunk_max: int = 4096, use_graph: bool = True):
     """Tracks every set to its budget in one batch; returns a list with one
     dict per set: x, px, y, py (final) and steps (survival turns)."""
     b = C.Batch(sets)
@@ -75,3 +82,92 @@ def run_sweep(sets, coords, arith: int = C.ARITH_EXACT, per_thread: int = 1,
         out.append({k: v[o:o + n] for k, v in fields.items()})
         o += n
     return out
+
+
+# ---- the reference's job list ------------------------------------------------------
+
+def read_jobs(path):
+    """Jobs of a compose_config.py list (htcondor_jobs/compose_config.py:12-15):
+    one "omega_x omega_y epsilon mu max_radius" line each."""
+    jobs = []
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if not parts:
+                continue
+            if len(parts) != 5:
+                raise ValueError(f"{path}: expected 5 numbers per line, got {line.strip()!r}")
+            ox, oy, eps, mu, rmax = (float(v) for v in parts)
+            jobs.append(dict(omega_x=ox, omega_y=oy, epsilon=eps, mu=mu, max_radius=rmax))
+    return jobs
+
+
+def job_grid(max_radius: float, num_points: int):
+    """run_sim.py's initial conditions (htcondor_jobs/run_sim.py:28-36): the
+    num_points x num_points grid of (x, y) on [0, max_radius]^2, px = py = 0."""
+    positions = np.linspace(0, max_radius, num_points)
+    xx, yy = np.meshgrid(positions, positions)
+    x, y = xx.flatten(), yy.flatten()
+    return x, np.zeros_like(x), y, np.zeros_like(y)
+
+
+def job_file_name(job) -> str:
+    """run_sim.py's output name (:64-66), decimal points written as "d"."""
+    f = lambda v: str(v).replace(".", "d")  # noqa: E731
+    return (f"stability_henon_{f(job['omega_x'])}_{f(job['omega_y'])}_{f(job['epsilon'])}_"
+            f"{f(job['mu'])}_{f(job['max_radius'])}")
+
+
+def run_jobs(jobs, num_points: int = 100, num_iterations: int = 100_000, out_dir=None,
+             arith: int = C.ARITH_EXACT):
+    """Every job of the list in one batch: SPS modulation, barrier 10, each on
+    its own grid (run_sim.py:40-47).  Returns the survival turns of each job;
+    with out_dir, also writes one file per job holding `steps`: HDF5 as the
+    reference does when h5py is importable, else .npz."""
+    import os
+
+    sets, pts = [], []
+    for j in jobs:
+        sets.append(dict(omega_x=j["omega_x"], omega_y=j["omega_y"], epsilon=j["epsilon"],
+                         mu=j["mu"], n_particles=num_points * num_points,
+                         n_turns=num_iterations, barrier=10.0))
+        pts.append(job_grid(j["max_radius"], num_points))
+    coords = tuple(np.concatenate([p[k] for p in pts]) for k in range(4)) if pts else \
+        tuple(np.zeros(0) for _ in range(4))
+    results = run_sweep(sets, coords, arith=arith) if sets else []
+    steps = [r["steps"] for r in results]
+    if out_dir is not None:
+        os.makedirs(out_dir, exist_ok=True)
+        try:
+            import h5py  # noqa: PLC0415
+        except ImportError:
+            h5py = None
+        for j, st in zip(jobs, steps):
+            base = os.path.join(out_dir, job_file_name(j))
+            if h5py is not None:
+                with h5py.File(base + ".h5", "w") as f:
+                    f.create_dataset("steps", data=st)
+            else:
+                np.savez(base + ".npz", steps=st)
+    return steps
+
+
+def main(argv=None) -> None:
+    import argparse
+    import time
+
+    ap = argparse.ArgumentParser(description="Run a job list of parameter sets as one batch.")
+    ap.add_argument("--jobs", required=True, help="compose_config.py list: omega_x omega_y "
+                                                  "epsilon mu max_radius per line")
+    ap.add_argument("--num_points", type=int, default=100)
+    ap.add_argument("--num_iterations", type=int, default=100_000)
+    ap.add_argument("--out", default=".")
+    args = ap.parse_args(argv)
+    jobs = read_jobs(args.jobs)
+    t0 = time.perf_counter()
+    run_jobs(jobs, args.num_points, args.num_iterations, args.out)
+    print(f"{len(jobs)} jobs in {time.perf_counter() - t0:.3f} s", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -145,3 +145,33 @@ def test_batch_groups_do_not_change_results(gpu):
     for bad in (-1.0, float("inf"), float("nan")):
         with pytest.raises(C.HMError):
             b.set_grid_share(bad)
+
+
+def test_job_list_runs_as_one_batch_like_run_sim(gpu, tmp_path):
+    # The reference runs each line of the job list as its own process
+    # (htcondor_jobs/run_sim.py); one batch must give every job the
+    # survival turns that script gets through the same facade calls.
+    import henon_map_cpp_b200 as hm
+
+    path = tmp_path / "all_jobs.txt"
+    path.write_text("0.168 0.201 0.0 0.0 0.75\n0.168 0.201 16.0 0.5 0.75\n"
+                    "0.31 0.32 64.0 0.25 0.25\n")
+    jobs = sweep.read_jobs(path)
+    n_points, n_iter = 12, 800
+    steps = sweep.run_jobs(jobs, n_points, n_iter, out_dir=tmp_path / "out")
+    for j, st in zip(jobs, steps):
+        x, px, y, py = sweep.job_grid(j["max_radius"], n_points)
+        p = hm.particles(x, px, y, py)
+        t = hm.henon_tracker(n_iter, j["omega_x"], j["omega_y"], "sps", epsilon=j["epsilon"])
+        t.track(p, n_iter, mu=j["mu"], barrier=10.0)
+        want = np.asarray(p.get_steps())
+        np.testing.assert_array_equal(st, want)
+        base = tmp_path / "out" / sweep.job_file_name(j)
+        h5, npz = base.with_suffix(".h5"), base.with_suffix(".npz")
+        if h5.exists():
+            import h5py
+
+            with h5py.File(h5, "r") as f:
+                np.testing.assert_array_equal(f["steps"][...], want)
+        else:
+            np.testing.assert_array_equal(np.load(npz)["steps"], want)
