@@ -5,10 +5,12 @@
 // reference's GPU classes (particles_4d_gpu, henon_tracker_gpu,
 // matrix_4d_vector_gpu, vector_4d_gpu, the constructs, storage_4d_gpu).
 // Long calls release the GIL; Ctrl-C stops them between turn chunks.
+#include <pybind11/eval.h>
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <array>
 #include <cmath>
 #include <limits>
 #include <stdexcept>
@@ -305,6 +307,43 @@ PYBIND11_MODULE(henon_map_engine, m) {
         return out;
     }, py::arg("x"), py::arg("px"), py::arg("y"), py::arg("py"), py::arg("from_idx"),
        py::arg("to_idx"), py::arg("method"));
+    // get_tunes (src/dynamic_indicator.cpp:333-362, bound at src/bind.cpp:241):
+    // (FFT tune, Birkhoff tune) of one plane's orbit over all its samples,
+    // i.e. the window [0, n-1] of the windowed tunes; NaN when the orbit
+    // holds a NaN.
+    m.def("get_tunes", [](std::vector<double> x, std::vector<double> px) {
+        if (x.size() != px.size())
+            throw std::runtime_error("get_tunes: x and px must be of the same size");
+        if (x.size() < 2) throw py::value_error("get_tunes: need at least two samples");
+        const uint32_t from = 0u, to = uint32_t(x.size() - 1);
+        double fft[4], birk[4];
+        check(hm_orbit_tunes_host(x.data(), px.data(), x.data(), px.data(), 1, x.size(), &from, &to,
+                                  1, 1, fft));
+        check(hm_orbit_tunes_host(x.data(), px.data(), x.data(), px.data(), 1, x.size(), &from, &to,
+                                  1, 0, birk));
+        return std::array<double, 2>{fft[0], birk[0]};
+    }, py::arg("x"), py::arg("px"));
+    // The reference's CPU classes (particles_4d, henon_tracker,
+    // matrix_4d_vector, storage_4d; src/bind.cpp:243-557) exist here by name,
+    // so that code importing them -- the reference's own Python package
+    // among it -- keeps working.  This build is the GPU path: constructing
+    // one raises, as the facade's force_CPU does; use the _gpu classes.
+    py::exec(R"(
+class _CpuClassNotProvided:
+    _name = ''
+    def __init__(self, *args, **kwargs):
+        raise NotImplementedError(
+            self._name + ': the CPU classes are not provided by this build; '
+            'use ' + self._name + '_gpu (bit-identical results on the GPU)')
+class particles_4d(_CpuClassNotProvided):
+    _name = 'particles_4d'
+class henon_tracker(_CpuClassNotProvided):
+    _name = 'henon_tracker'
+class matrix_4d_vector(_CpuClassNotProvided):
+    _name = 'matrix_4d_vector'
+class storage_4d(_CpuClassNotProvided):
+    _name = 'storage_4d'
+)", m.attr("__dict__"));
     m.def("birkhoff_weights", [](unsigned n) {
         auto out = array1<double>(n);
         check(hm_birkhoff_weights(n, out.mutable_data()));

@@ -49,3 +49,24 @@ def test_no_silent_cpu_fallback():
         hm.henon_tracker(10, 0.1, 0.2, "sps")
     with pytest.raises(NotImplementedError):
         hm.henon_tracker(10, 0.1, 0.2, "sps", force_CPU=True)
+
+
+def test_engine_has_every_name_the_reference_package_imports():
+    # henon_map_cpp/__init__.py:5-17 imports these from its engine; the
+    # module-level functions are those of src/bind.cpp:227-242.
+    from henon_map_cpp_b200 import henon_map_engine as E
+
+    for name in ("birkhoff_weights", "henon_tracker", "henon_tracker_gpu",
+                 "lyapunov_birkhoff_construct", "lyapunov_birkhoff_construct_multi",
+                 "matrix_4d_vector", "matrix_4d_vector_gpu", "megno_birkhoff_construct",
+                 "megno_construct", "particles_4d", "particles_4d_gpu", "storage_4d",
+                 "storage_4d_gpu", "tune_birkhoff_construct", "vector_4d_gpu",
+                 "is_cuda_device_available", "basic_modulation", "sps_modulation",
+                 "gaussian_modulation", "uniform_modulation", "get_tunes"):
+        assert hasattr(E, name), name
+    # The CPU classes exist by name only: this build is the GPU path.
+    for cls, args in ((E.particles_4d, ([0.0], [0.0], [0.0], [0.0])),
+                      (E.henon_tracker, (10, 0.1, 0.2, "sps", 0.0, 0.0, 0)),
+                      (E.matrix_4d_vector, (4,)), (E.storage_4d, (4,))):
+        with pytest.raises(NotImplementedError, match="_gpu"):
+            cls(*args)

@@ -118,3 +118,22 @@ def test_tracker_megno_equals_construct_loop(gpu):
     assert_bitwise(got[:, 0], snaps[100])
     assert_bitwise(got[:, 1], snaps[500])
     assert np.isfinite(got[:, 1]).any() and np.isnan(got[:, 1]).any()
+
+
+def test_engine_get_tunes_matches_oracle(gpu):
+    # get_tunes(x, px) of the engine (src/dynamic_indicator.cpp:333-362):
+    # (FFT tune, Birkhoff tune) of one plane's whole orbit.
+    from henon_map_cpp_b200 import henon_map_engine as E
+
+    x, px, y, py = grid(0.3, 3)
+    orb = T.orbit(x, px, y, py, O.tables(2000, *TUNES, "sps", epsilon=16.0), 2000, 0.2)
+    for i in range(x.size):
+        q, p = orb[0][:, i], orb[1][:, i]
+        fft, birk = E.get_tunes(q, p)
+        np.testing.assert_allclose(birk, T.birkhoff_tune(q, p), rtol=1e-13)
+        np.testing.assert_allclose(fft, T.fft_tune(q, p), rtol=1e-10)
+    q = orb[0][:, 0].copy()
+    q[7] = np.nan
+    assert np.all(np.isnan(E.get_tunes(q, orb[1][:, 0])))
+    with pytest.raises(RuntimeError, match="same size"):
+        E.get_tunes(orb[0][:10, 0], orb[1][:9, 0])
