@@ -29,12 +29,6 @@ namespace {
 
 using dev::Rn;
 
-// r < barrier^2 on the radius the loss uses (see dev::Barrier for the
-// bit-pattern compare).
-__device__ __forceinline__ bool inside(double r, long long b2bits) {
-    return dev::pattern(r) < static_cast<unsigned long long>(b2bits);
-}
-
 struct S4 {
     double x, px, y, py;
 };
@@ -45,7 +39,9 @@ struct S4 {
 // thread holds kPerThread doubles of the next stage in registers (plain
 // loads, issued a whole stage ahead of use) and stores them into the other
 // buffer at the end of the stage.  The launch often holds few warps per
-// SM, too few to hide per-turn L2 latency otherwise.
+// SM, too few to hide per-turn L2 latency otherwise.  (Blocks of 64 threads
+// balance a small launch better over the SMs but measured 2.6 % slower:
+// twice the staging registers per thread.)
 constexpr int kThreads = 128;
 constexpr uint32_t kStage = 64u;
 constexpr int kRec = 6;  // doubles per turn: sin wx, cos wx, sin wy, cos wy, w_k, S_k
@@ -73,15 +69,21 @@ __device__ __forceinline__ void rec_store(double *buf, const double (&r)[kPerThr
     for (int q = 0; q < kPerThread; ++q) buf[threadIdx.x + uint32_t(kThreads * q)] = r[q];
 }
 
-// One forward turn; returns x^2+px^2+y^2+py^2 of the new state in the
-// tracker's grouping (the loss uses the same number).
+// One forward turn of a particle held with its squares (dev::Particle, so
+// that x*x and y*y are not recomputed).  Sets `in` to the tracker's survival
+// decision (the same barrier test, bit for bit) and returns the radius the
+// loss uses: x^2+px^2+y^2+py^2 with two FMAs, within 2 ulp of the
+// separately rounded sum.
 template <int ARITH, bool OCT>
-__device__ __forceinline__ double fwd(S4 &s, const dev::Turn &t, double mu) {
-    dev::Particle p = dev::make_particle(s.x, s.px, s.y, s.py);
+__device__ __forceinline__ double fwd(dev::Particle &p, const dev::Turn &t, double mu,
+                                      const dev::Barrier &bar, bool &in) {
     dev::turn<ARITH, OCT, false>(p, t, mu);
-    s = S4{p.x, p.px, p.y, p.py};
-    return ARITH == HM_ARITH_EXACT ? dev::radius_exact(p) : dev::radius_fma(p);
+    const double r = dev::radius_fma(p);
+    in = dev::small_inside(p, bar) || dev::inside<ARITH>(r, p, bar);
+    return r;
 }
+
+__device__ __forceinline__ S4 coords(const dev::Particle &p) { return S4{p.x, p.px, p.y, p.py}; }
 
 __device__ __forceinline__ void store4(double *buf, size_t slot, size_t n, size_t i, const S4 &s) {
     double *b = buf + slot * 4 * n;
@@ -102,14 +104,16 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const AdjointArgs a) {
     if (i >= a.n) return;
     const size_t n = a.n;
     const uint32_t N = a.n_turns, C = a.ckpt;
-    S4 s{a.x0[i], a.px0[i], a.y0[i], a.py0[i]};
+    dev::Particle s = dev::make_particle(a.x0[i], a.px0[i], a.y0[i], a.py0[i]);
+    const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
     double loss = 0.0;
     uint32_t k = 0;
     for (; alive && k < N; ++k) {
-        if (k % C == 0) store4(a.ckpt_buf, k / C, n, i, s);
-        const double r = fwd<ARITH, OCT>(s, dev::load_turn(a.table, k), a.mu);
-        if (!inside(r, a.b2bits)) {
+        if (k % C == 0) store4(a.ckpt_buf, k / C, n, i, coords(s));
+        bool in;
+        const double r = fwd<ARITH, OCT>(s, dev::load_turn(a.table, k), a.mu, bar, in);
+        if (!in) {
             alive = false;
             break;
         }
@@ -134,10 +138,11 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const AdjointArgs a) {
     for (int seg = int(n_seg) - 1; seg >= 0; --seg) {
         const uint32_t k0 = uint32_t(seg) * C;
         const uint32_t len = min(C, N - k0);
-        S4 q = load4(a.ckpt_buf, uint32_t(seg), n, i);
+        const S4 c = load4(a.ckpt_buf, uint32_t(seg), n, i);
+        dev::Particle q = dev::make_particle(c.x, c.px, c.y, c.py);
         for (uint32_t j = 0; j < len; ++j) {
-            store4(a.seg_buf, j, n, i, q);
-            fwd<ARITH, OCT>(q, dev::load_turn(a.table, k0 + j), mu);
+            store4(a.seg_buf, j, n, i, coords(q));
+            dev::turn<ARITH, OCT, false>(q, dev::load_turn(a.table, k0 + j), mu);
         }
         for (int j = int(len) - 1; j >= 0; --j) {
             const uint32_t kk = k0 + uint32_t(j);
@@ -202,7 +207,8 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
     const size_t n = a.n;
     const uint32_t N = a.n_turns, C = a.ckpt;
     const uint32_t n_stages = (N + kStage - 1) / kStage;
-    S4 s{a.x0[ii], a.px0[ii], a.y0[ii], a.py0[ii]};
+    dev::Particle s = dev::make_particle(a.x0[ii], a.px0[ii], a.y0[ii], a.py0[ii]);
+    const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     bool alive = in_range && !dev::is_lost(s.x, s.px, s.y, s.py);
     double next[kPerThread];
 
@@ -220,19 +226,21 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
         const bool more = sg + 1 < n_stages;
         if (more) rec_load(next, a, k0 + kStage, min(kStage, N - k0 - kStage));
         const double *R = recs[sg & 1u];
-        for (uint32_t kk = 0; alive && kk < kn; ++kk) {
+        // No branch on the turn's result: a lost particle keeps turning to
+        // the end of the stage (its state, loss and checkpoints are never
+        // used), so that the next turn need not wait for the loss test.
+        for (uint32_t kk = 0; kk < kn; ++kk) {
             const uint32_t k = k0 + kk;
             if (k == next_ckpt) {
-                store4(a.ckpt_buf, k / C, n, i, s);
+                if (alive) store4(a.ckpt_buf, k / C, n, i, coords(s));
                 next_ckpt += C;
             }
             const double *rr = R + kRec * kk;
-            const double r = fwd<ARITH, OCT>(s, dev::Turn{rr[0], rr[1], rr[2], rr[3]}, a.mu);
-            if (!inside(r, a.b2bits)) {
-                alive = false;
-                lost_at = k;
-                break;
-            }
+            bool in;
+            const double r =
+                fwd<ARITH, OCT>(s, dev::Turn{rr[0], rr[1], rr[2], rr[3]}, a.mu, bar, in);
+            lost_at = (alive && !in) ? k : lost_at;
+            alive = alive && in;
             loss = fma(rr[4], r, loss);
         }
         // The other buffer was last read in the previous stage, which the
@@ -247,12 +255,15 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
     }
 
     // ---- reverse sweep: turns N-1 .. 0 --------------------------------------------
-    const double mu = a.mu;
+    // The sweep carries half the adjoint (lambda / 2, with w_k in place of
+    // 2 w_k in grad A); every quantity is linear in it, so the results are
+    // doubled, exactly, at the end.
+    const double mu = a.mu, mu6 = -6.0 * a.mu;
     double lx = 0.0, lpx = 0.0, ly = 0.0, lpy = 0.0;
     // sum_k gw_k and sum_k S_k gw_k per plane: the parameter gradients are
     // combined from them at the end.
     double Gx = 0.0, Gy = 0.0, Hx = 0.0, Hy = 0.0, g_mu = 0.0;
-    S4 post = s;  // the state after turn N-1
+    S4 post = coords(s);  // the state after turn N-1
     const uint32_t n_seg = (N + C - 1) / C;
     // Turns left in the current segment; at 0 the next (earlier) segment
     // starts from its stored end state, the checkpoint after it.
@@ -283,19 +294,20 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
                 // inverse turn (henon_step reverse order, src/henon.cu:510-528)
                 const double x = fma(t.cx, X, -t.sx * PX), px1 = fma(t.sx, X, t.cx * PX);
                 const double y = fma(t.cy, Y, -t.sy * PY), py1 = fma(t.sy, Y, t.cy * PY);
-                const double xx = x * x, yy = y * y;
+                const double xx = x * x, yy = y * y, xy = x * y;
                 const double dxy = xx - yy;
-                const double ax3 = fma(-3.0, yy, xx), ay3 = fma(-3.0, xx, yy);
-                double qx = dxy, qy = -2.0 * x * y;
+                // x (x^2 - 3y^2), y (y^2 - 3x^2): the octupole kicks over mu
+                const double xa = x * fma(-3.0, yy, xx), ya = y * fma(-3.0, xx, yy);
+                double qx = dxy, qy = -2.0 * xy;
                 if (OCT) {
-                    qx = fma(mu * x, ax3, qx);
-                    qy = fma(mu * y, ay3, qy);
+                    qx = fma(mu, xa, qx);
+                    qy = fma(mu, ya, qy);
                 }
                 post = S4{x, px1 - qx, y, py1 - qy};
-                // adjoint of the post-turn state: lambda + w_k grad A
-                const double w2 = 2.0 * rr[4];
-                const double aX = fma(w2, X, lx), aPX = fma(w2, PX, lpx);
-                const double aY = fma(w2, Y, ly), aPY = fma(w2, PY, lpy);
+                // adjoint of the post-turn state: (lambda + 2 w_k grad A) / 2
+                const double w = rr[4];
+                const double aX = fma(w, X, lx), aPX = fma(w, PX, lpx);
+                const double aY = fma(w, Y, ly), aPY = fma(w, PY, lpy);
                 const double gwx = fma(aX, PX, -aPX * X);
                 const double gwy = fma(aY, PY, -aPY * Y);
                 const double Sk = rr[5];
@@ -305,14 +317,16 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
                 Hy = fma(Sk, gwy, Hy);
                 const double rx = fma(t.cx, aX, -t.sx * aPX), rpx = fma(t.sx, aX, t.cx * aPX);
                 const double ry = fma(t.cy, aY, -t.sy * aPY), rpy = fma(t.sy, aY, t.cy * aPY);
-                double da = 2.0 * x, db = -2.0 * y, dd = -2.0 * x;
+                double da = 2.0 * x, db = -2.0 * y;
                 if (OCT) {
                     da = fma(3.0 * mu, dxy, da);
-                    db = fma(-6.0 * mu * x, y, db);
-                    dd = fma(-3.0 * mu, dxy, dd);
+                    db = fma(mu6, xy, db);
                 }
+                // d(py1)/dy = -2x (- 3 mu (x^2 - y^2)) = -da exactly, since
+                // fma(-a, b, -c) = -fma(a, b, c).
+                const double dd = -da;
                 // d(px1, py1)/d mu = (x (x^2 - 3y^2), y (y^2 - 3x^2)), also at mu = 0
-                g_mu = fma(rpx, x * ax3, fma(rpy, y * ay3, g_mu));
+                g_mu = fma(rpx, xa, fma(rpy, ya, g_mu));
                 lx = fma(rpx, da, fma(rpy, db, rx));
                 ly = fma(rpx, db, fma(rpy, dd, ry));
                 lpx = rpx;
@@ -328,15 +342,15 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
         a.g_th[i] = a.g_th[n + i] = a.g_th[2 * n + i] = a.g_th[3 * n + i] = 0.0;
         return;
     }
-    a.g_ic[i] = lx;
-    a.g_ic[n + i] = lpx;
-    a.g_ic[2 * n + i] = ly;
-    a.g_ic[3 * n + i] = lpy;
+    a.g_ic[i] = 2.0 * lx;
+    a.g_ic[n + i] = 2.0 * lpx;
+    a.g_ic[2 * n + i] = 2.0 * ly;
+    a.g_ic[3 * n + i] = 2.0 * lpy;
     // omega(k) = omega0 (1 + eps S_k): d/d omega0 = 1 + eps S_k, d/d eps = omega0 S_k
-    a.g_th[i] = fma(a.epsilon, Hx, Gx);
-    a.g_th[n + i] = fma(a.epsilon, Hy, Gy);
-    a.g_th[2 * n + i] = fma(a.omega_x0, Hx, a.omega_y0 * Hy);
-    a.g_th[3 * n + i] = g_mu;
+    a.g_th[i] = 2.0 * fma(a.epsilon, Hx, Gx);
+    a.g_th[n + i] = 2.0 * fma(a.epsilon, Hy, Gy);
+    a.g_th[2 * n + i] = 2.0 * fma(a.omega_x0, Hx, a.omega_y0 * Hy);
+    a.g_th[3 * n + i] = 2.0 * g_mu;
 }
 
 // Forward mode: loss and, with TANGENT, g = sum_k w_k M_{k+1}^T grad A(x_{k+1})
@@ -346,7 +360,8 @@ __global__ void __launch_bounds__(128) forward_loss_kernel(const AdjointArgs a) 
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const size_t n = a.n;
-    S4 s{a.x0[i], a.px0[i], a.y0[i], a.py0[i]};
+    dev::Particle s = dev::make_particle(a.x0[i], a.px0[i], a.y0[i], a.py0[i]);
+    const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
     double M[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
     double g[4] = {0, 0, 0, 0};
@@ -369,8 +384,9 @@ __global__ void __launch_bounds__(128) forward_loss_kernel(const AdjointArgs a) 
 #pragma unroll
             for (int q = 0; q < 16; ++q) M[q] = out[q];
         }
-        const double r = fwd<ARITH, OCT>(s, t, a.mu);
-        if (!inside(r, a.b2bits)) {
+        bool in;
+        const double r = fwd<ARITH, OCT>(s, t, a.mu, bar, in);
+        if (!in) {
             alive = false;
             break;
         }
@@ -400,8 +416,9 @@ cudaError_t launch_a(const AdjointArgs &a, int mode, cudaStream_t s) {
         if (oct) adjoint_kernel<ARITH, true><<<blocks, 128, 0, s>>>(a);
         else adjoint_kernel<ARITH, false><<<blocks, 128, 0, s>>>(a);
     } else if (mode == 3) {
-        if (oct) adjoint_inverse_kernel<ARITH, true><<<blocks, kThreads, 0, s>>>(a);
-        else adjoint_inverse_kernel<ARITH, false><<<blocks, kThreads, 0, s>>>(a);
+        const unsigned b = unsigned((a.n + kThreads - 1) / kThreads);
+        if (oct) adjoint_inverse_kernel<ARITH, true><<<b, kThreads, 0, s>>>(a);
+        else adjoint_inverse_kernel<ARITH, false><<<b, kThreads, 0, s>>>(a);
     } else if (mode == 1) {
         if (oct) forward_loss_kernel<ARITH, true, true><<<blocks, 128, 0, s>>>(a);
         else forward_loss_kernel<ARITH, false, true><<<blocks, 128, 0, s>>>(a);

@@ -113,7 +113,7 @@ __global__ void batch_plan_kernel(BatchDev b, uint32_t chunk_len_done, uint32_t 
 template <int ARITH, bool OCT, int K>
 __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &set,
                                          const BatchStateDev &st, uint32_t s, uint32_t start,
-                                         int in, int out, double *bufs) {
+                                         int in, int out, double *bufs, double2 *ckpt) {
     const unsigned lane = threadIdx.x & 31u;
     Particle p[K];
     uint64_t id[K];
@@ -149,8 +149,37 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
             stage_load(next, set.table, turn0 + k0 + kStageTurns,
                        min(kStageTurns, nt - k0 - kStageTurns), lane);
         const double *rec = bufs + (sg & 1u) * kStageTurns * 4u;
-#pragma unroll 2
-        for (uint32_t kk = 0; warp_live && kk < kn_stage; ++kk) {
+        // The stage's turns with no per-turn control flow, ORing every
+        // coordinate's high word; one vote at the end.  Only a warp with a
+        // coordinate at or above the bound of dev::small_or restores the
+        // saved particles and redoes the stage with the per-turn test
+        // (the scheme of the tracking kernel, track.cu turns_staged).
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            ckpt[2 * (j * 32 + int(lane))] = make_double2(p[j].x, p[j].px);
+            ckpt[2 * (j * 32 + int(lane)) + 1] = make_double2(p[j].y, p[j].py);
+        }
+        uint32_t ored_stage = 0u;
+        for (uint32_t kk = 0; kk < kn_stage; ++kk) {
+            const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * kk);
+            const double2 q0 = q[0], q1 = q[1];
+            const dev::Turn t{q0.x, q0.y, q1.x, q1.y};
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                dev::turn<ARITH, OCT, false>(p[j], t, mu);
+                ored_stage |= dev::hi_or(p[j]);
+            }
+        }
+        const bool redo = __any_sync(dev::kFullMask, !dev::small_or(ored_stage, bar));
+        if (redo) {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                const double2 a = ckpt[2 * (j * 32 + int(lane))];
+                const double2 c = ckpt[2 * (j * 32 + int(lane)) + 1];
+                p[j] = dev::make_particle(a.x, a.y, c.x, c.y);
+            }
+        }
+        for (uint32_t kk = 0; redo && warp_live && kk < kn_stage; ++kk) {
             const uint32_t k = k0 + kk;
             const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * kk);
             const double2 q0 = q[0], q1 = q[1];
@@ -219,8 +248,11 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
 template <int ARITH, int K>
 __global__ void __launch_bounds__(kThreads, K == 1 ? 7 : 1) batch_chunk_kernel(BatchDev b) {
     __shared__ __align__(16) double stage_bufs[kWarps][2 * kStageTurns * 4];
+    // Per warp, the particles {x, px}, {y, py} at the start of a stage.
+    __shared__ __align__(16) double2 checkpoints[kWarps][2 * 32 * K];
     const unsigned lane = threadIdx.x & 31u;
     double *bufs = stage_bufs[threadIdx.x >> 5];
+    double2 *ckpt = checkpoints[threadIdx.x >> 5];
     const uint32_t n_tiles = *b.n_tiles;
     const int in = int(*b.parity), out = 1 - in;
     while (true) {
@@ -233,9 +265,9 @@ __global__ void __launch_bounds__(kThreads, K == 1 ? 7 : 1) batch_chunk_kernel(B
         const BatchSetDev &set = b.sets[s];
         const uint32_t start = (item - st.first_tile) * 32u * uint32_t(K);
         if (set.mu != 0.0)
-            run_tile<ARITH, true, K>(b, set, st, s, start, in, out, bufs);
+            run_tile<ARITH, true, K>(b, set, st, s, start, in, out, bufs, ckpt);
         else
-            run_tile<ARITH, false, K>(b, set, st, s, start, in, out, bufs);
+            run_tile<ARITH, false, K>(b, set, st, s, start, in, out, bufs, ckpt);
     }
 }
 

@@ -98,6 +98,23 @@ __device__ __forceinline__ void turns_direct(const TrackChunk &c, const Barrier 
     }
 }
 
+// Turns between two barrier votes of the staged kernel (see turns_staged).
+constexpr uint32_t kCheckTurns = 32;
+
+// Shared memory of a staged launch: two stage buffers of turn records and,
+// without kicks, one checkpoint {x, px, y, py} per particle.
+__host__ __device__ constexpr size_t staged_smem_bytes(uint32_t stage_turns, uint32_t threads,
+                                                       int per_thread, bool kick) {
+    return size_t(stage_turns) * 2u * 32u + (kick ? 0u : size_t(threads) * per_thread * 32u);
+}
+
+__device__ __forceinline__ Turn staged_record(const double *rec, uint32_t kn, uint32_t kk,
+                                              bool rev) {
+    const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * (rev ? kn - 1u - kk : kk));
+    const double2 a = q[0], b = q[1];
+    return Turn{a.x, a.y, b.x, b.y};
+}
+
 // The chunk's turns with the turn records staged in shared memory: the
 // chunk is cut into stages of c.stage_turns turns whose records (a
 // contiguous span of the table) one thread brings in with a bulk copy,
@@ -105,17 +122,30 @@ __device__ __forceinline__ void turns_direct(const TrackChunk &c, const Barrier 
 // stage s.  Every warp then reads each record from shared memory as a
 // broadcast.  Warps whose particles are all lost keep taking part in the
 // per-stage barriers; the block stops when none of its warps is live.
+//
+// Without kicks, a stage runs in runs of kCheckTurns turns with no
+// per-turn control flow: the thread saves its particles to shared memory,
+// applies the turns while ORing every coordinate's high word, and the warp
+// votes once at the end.  If no coordinate of any turn reached the bound
+// of dev::small_or, no particle can have been lost in the run, which is
+// then exactly what the per-turn test would have produced.  Otherwise the
+// warp restores the saved particles and redoes the run with the per-turn
+// test (turn_all), which finds the loss turn.  A per-turn vote made each
+// turn wait for the tail of the previous one; a redo costs one run per
+// loss event of a warp.
 // Returns false when a copy did not land within the bounded wait (the
 // chunk's results are then invalid and c.fault is set).
 template <int ARITH, bool OCT, bool REV, int K, bool KICK>
 __device__ __forceinline__ bool turns_staged(const TrackChunk &c, const Barrier &bar,
                                              Particle (&p)[K], const uint32_t (&id)[K],
                                              bool (&live)[K], bool warp_live) {
-    extern __shared__ __align__(128) double stage_buf[];  // [2][S][4]
+    // [2][S][4] turn records, then (no kicks) [K][blockDim.x] checkpoints.
+    extern __shared__ __align__(128) double stage_buf[];
     __shared__ __align__(8) uint64_t full[2];
     const double mu = c.mu;
     const uint32_t nt = c.n_turns, S = c.stage_turns;
     const uint32_t n_stages = (nt + S - 1) / S;
+    double2 *const ckpt = reinterpret_cast<double2 *>(stage_buf + size_t(S) * 8u);
     const bool leader = threadIdx.x == 0;
     auto issue = [&](uint32_t st) {
         const uint32_t k0 = st * S;
@@ -144,15 +174,41 @@ __device__ __forceinline__ bool turns_staged(const TrackChunk &c, const Barrier 
         const uint32_t k0 = st * S;
         const uint32_t kn = min(S, nt - k0);
         const double *rec = stage_buf + size_t(buf) * S * 4u;
-        if (!timed_out) {
-            // Two turns per iteration: 1.4 points of FP64 peak over one
-            // (exact arithmetic, two particles per thread).
+        if (!timed_out && KICK) {
 #pragma unroll 2
-            for (uint32_t kk = 0; warp_live && kk < kn; ++kk) {
-                const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * (REV ? kn - 1u - kk : kk));
-                const double2 a = q[0], b = q[1];
-                turn_all<ARITH, OCT, REV, K, KICK>(c, bar, mu, Turn{a.x, a.y, b.x, b.y}, k0 + kk, p,
-                                                   id, live, warp_live);
+            for (uint32_t kk = 0; warp_live && kk < kn; ++kk)
+                turn_all<ARITH, OCT, REV, K, KICK>(c, bar, mu, staged_record(rec, kn, kk, REV),
+                                                   k0 + kk, p, id, live, warp_live);
+        } else if (!timed_out) {
+            for (uint32_t j0 = 0; warp_live && j0 < kn; j0 += kCheckTurns) {
+                const uint32_t j1 = min(j0 + kCheckTurns, kn);
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    ckpt[2u * (j * blockDim.x + threadIdx.x)] = make_double2(p[j].x, p[j].px);
+                    ckpt[2u * (j * blockDim.x + threadIdx.x) + 1u] = make_double2(p[j].y, p[j].py);
+                }
+                uint32_t ored = 0u;
+#pragma unroll 2
+                for (uint32_t kk = j0; kk < j1; ++kk) {
+                    const Turn t = staged_record(rec, kn, kk, REV);
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        dev::turn<ARITH, OCT, REV>(p[j], t, mu);
+                        ored |= dev::hi_or(p[j]);
+                    }
+                }
+                if (__any_sync(kFullMask, !dev::small_or(ored, bar))) {
+#pragma unroll
+                    for (int j = 0; j < K; ++j) {
+                        const double2 a = ckpt[2u * (j * blockDim.x + threadIdx.x)];
+                        const double2 b = ckpt[2u * (j * blockDim.x + threadIdx.x) + 1u];
+                        p[j] = dev::make_particle(a.x, a.y, b.x, b.y);
+                    }
+                    for (uint32_t kk = j0; warp_live && kk < j1; ++kk)
+                        turn_all<ARITH, OCT, REV, K, KICK>(c, bar, mu,
+                                                           staged_record(rec, kn, kk, REV),
+                                                           k0 + kk, p, id, live, warp_live);
+                }
             }
         }
         // Every warp is done with this buffer (and knows whether any warp of
@@ -180,11 +236,8 @@ __device__ __forceinline__ bool turns_staged(const TrackChunk &c, const Barrier 
 }
 
 // One chunk of turns for the particles of one block (K per thread).
-// At most two particles per thread the kernel fits 64 registers without
-// spills, i.e. 8 blocks of 128 threads per SM; four per thread need more.
 template <int ARITH, bool OCT, bool REV, int K, bool STAGED, bool KICK>
-__global__ void __launch_bounds__(256, K <= 2 ? 4 : 1)
-track_chunk_kernel(const TrackChunk c) {
+__device__ __forceinline__ void track_chunk(const TrackChunk &c) {
     const uint32_t n_in = c.in_count ? *c.in_count : c.n_user;
     const uint32_t base = blockIdx.x * (blockDim.x * K);
     if (base >= n_in) return;  // whole block past the list
@@ -268,13 +321,36 @@ track_chunk_kernel(const TrackChunk c) {
     }
 }
 
+// At most two particles per thread the kernel fits 64 registers without
+// spills, i.e. 8 blocks of 128 threads per SM; four per thread need more.
+template <int ARITH, bool OCT, bool REV, int K, bool STAGED, bool KICK>
+__global__ void __launch_bounds__(256, K <= 2 ? 4 : 1) track_chunk_kernel(const TrackChunk c) {
+    track_chunk<ARITH, OCT, REV, K, STAGED, KICK>(c);
+}
+
+// Staged fast arithmetic with two particles per thread, capped at 56
+// registers (9 blocks of 128 threads per SM): 76.5 % of the FP64 peak on
+// the DA scan against 74.5 % at 64.  Exact arithmetic gains nothing there.
+template <int ARITH, bool OCT, bool REV>
+__global__ void __maxnreg__(56) track_chunk_kernel_r56(const TrackChunk c) {
+    track_chunk<ARITH, OCT, REV, 2, true, false>(c);
+}
+
 template <int ARITH, bool OCT, bool REV, int K, bool KICK>
 cudaError_t launch_s(const TrackChunk &c, unsigned blocks, int threads, cudaStream_t s) {
     if (c.stage_turns == 0) {
         track_chunk_kernel<ARITH, OCT, REV, K, false, KICK><<<blocks, threads, 0, s>>>(c);
     } else {
-        const size_t smem = size_t(c.stage_turns) * 2u * 32u;
-        track_chunk_kernel<ARITH, OCT, REV, K, true, KICK><<<blocks, threads, smem, s>>>(c);
+        const size_t smem = staged_smem_bytes(c.stage_turns, uint32_t(threads), K, KICK);
+        auto kernel = track_chunk_kernel<ARITH, OCT, REV, K, true, KICK>;
+        if constexpr (ARITH == HM_ARITH_FAST && K == 2 && !KICK)
+            kernel = track_chunk_kernel_r56<ARITH, OCT, REV>;
+        if (smem > 48u * 1024u) {
+            const cudaError_t e =
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (e != cudaSuccess) return e;
+        }
+        kernel<<<blocks, threads, smem, s>>>(c);
     }
     return cudaGetLastError();
 }
