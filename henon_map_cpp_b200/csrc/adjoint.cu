@@ -210,6 +210,8 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
     dev::Particle s = dev::make_particle(a.x0[ii], a.px0[ii], a.y0[ii], a.py0[ii]);
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     bool alive = in_range && !dev::is_lost(s.x, s.px, s.y, s.py);
+    // Particles out of the game hold zeros, a fixed point of the map.
+    if (!alive) s = dev::make_particle(0.0, 0.0, 0.0, 0.0);
     double next[kPerThread];
 
     // ---- forward sweep: loss and checkpoints ----------------------------------
@@ -226,9 +228,16 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
         const bool more = sg + 1 < n_stages;
         if (more) rec_load(next, a, k0 + kStage, min(kStage, N - k0 - kStage));
         const double *R = recs[sg & 1u];
-        // No branch on the turn's result: a lost particle keeps turning to
-        // the end of the stage (its state, loss and checkpoints are never
-        // used), so that the next turn need not wait for the loss test.
+        // The stage's turns with no branch on their results (the tracking
+        // kernel's scheme, track.cu turns_staged): the loss accumulates and
+        // every coordinate's high word is ORed; one warp vote at the end.
+        // Only a warp with a coordinate at or above the bound of
+        // dev::small_or (so possibly a loss) restores the stage's start and
+        // redoes it with the per-turn test, which finds the loss turn.
+        const dev::Particle s0 = s;
+        const double loss0 = loss;
+        const uint32_t ckpt0 = next_ckpt;
+        uint32_t ored = 0u;
         for (uint32_t kk = 0; kk < kn; ++kk) {
             const uint32_t k = k0 + kk;
             if (k == next_ckpt) {
@@ -236,12 +245,31 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
                 next_ckpt += C;
             }
             const double *rr = R + kRec * kk;
-            bool in;
-            const double r =
-                fwd<ARITH, OCT>(s, dev::Turn{rr[0], rr[1], rr[2], rr[3]}, a.mu, bar, in);
-            lost_at = (alive && !in) ? k : lost_at;
-            alive = alive && in;
-            loss = fma(rr[4], r, loss);
+            dev::turn<ARITH, OCT, false>(s, dev::Turn{rr[0], rr[1], rr[2], rr[3]}, a.mu);
+            loss = fma(rr[4], dev::radius_fma(s), loss);
+            ored |= dev::hi_or(s);
+        }
+        if (__any_sync(dev::kFullMask, !dev::small_or(ored, bar))) {
+            s = s0;
+            loss = loss0;
+            next_ckpt = ckpt0;
+            for (uint32_t kk = 0; kk < kn; ++kk) {
+                const uint32_t k = k0 + kk;
+                if (k == next_ckpt) {
+                    if (alive) store4(a.ckpt_buf, k / C, n, i, coords(s));
+                    next_ckpt += C;
+                }
+                const double *rr = R + kRec * kk;
+                bool in;
+                const double r =
+                    fwd<ARITH, OCT>(s, dev::Turn{rr[0], rr[1], rr[2], rr[3]}, a.mu, bar, in);
+                loss = fma(rr[4], r, loss);
+                if (alive && !in) {
+                    lost_at = k;
+                    alive = false;
+                    s = dev::make_particle(0.0, 0.0, 0.0, 0.0);
+                }
+            }
         }
         // The other buffer was last read in the previous stage, which the
         // whole block has finished; the barrier publishes the stores.
@@ -268,6 +296,10 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
     // Turns left in the current segment; at 0 the next (earlier) segment
     // starts from its stored end state, the checkpoint after it.
     uint32_t seg_left = N - (n_seg ? n_seg - 1u : 0u) * C;
+    // The end state of the next (earlier) segment, loaded one segment ahead
+    // of its use.
+    S4 pre{0.0, 0.0, 0.0, 0.0};
+    if (alive && n_seg > 1u) pre = load4(a.ckpt_buf, n_seg - 1u, n, i);
     if (__syncthreads_or(alive) && n_stages > 0) {
         rec_load(next, a, N - min(kStage, N), min(kStage, N));
         rec_store(recs[0], next);
@@ -284,7 +316,9 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
             for (uint32_t j = 0; alive && j < kn; ++j) {
                 const uint32_t kk = N - 1u - (k0 + j);  // turn index, descending
                 if (seg_left == 0u) {
-                    post = load4(a.ckpt_buf, (kk + 1u) / C, n, i);
+                    post = pre;
+                    const uint32_t idx = (kk + 1u) / C;
+                    if (idx > 1u) pre = load4(a.ckpt_buf, idx - 1u, n, i);
                     seg_left = C;
                 }
                 --seg_left;

@@ -345,7 +345,10 @@ cudaError_t launch_s(const TrackChunk &c, unsigned blocks, int threads, cudaStre
         auto kernel = track_chunk_kernel<ARITH, OCT, REV, K, true, KICK>;
         if constexpr (ARITH == HM_ARITH_FAST && K == 2 && !KICK)
             kernel = track_chunk_kernel_r56<ARITH, OCT, REV>;
-        if (smem > 48u * 1024u) {
+        // Dynamic plus static shared memory above 48 KB needs the opt-in
+        // (the kernel's static part is its two mbarriers): 256 threads with
+        // four particles each and 256-turn stages take exactly 48 KB dynamic.
+        if (smem > 40u * 1024u) {
             const cudaError_t e =
                 cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             if (e != cudaSuccess) return e;
