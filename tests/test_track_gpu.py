@@ -211,11 +211,15 @@ def test_launch_shape_does_not_change_results(gpu):
         C.set_track_config(*saved)
 
 
-@pytest.mark.parametrize("stage", [16, 128, 512])
+@pytest.mark.parametrize("stage", [16, 128, 256, 512])
 def test_staged_turn_records_give_identical_results(gpu, stage):
     # Turn records brought into shared memory by bulk copies, stage by
     # stage: chunk lengths that are not multiples of the stage, one to four
-    # particles per thread, forward and reverse.
+    # particles per thread, forward and reverse.  Stages of 16 turns are
+    # shorter than the kernel's 32-turn runs between barrier votes; 256
+    # turns with 256 threads of four particles take exactly 48 KB of
+    # dynamic shared memory (records plus checkpoints), past the limit
+    # without the opt-in.
     x, px, y, py = grid(0.6, 40)
     ref = run_oracle(x, px, y, py, 2500, 64.0, 0.2)
     saved, saved_stage = C.get_track_config(), C.get_track_staging()
