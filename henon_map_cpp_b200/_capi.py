@@ -98,6 +98,7 @@ _SIGNATURES = {
     "hm_track_device_noalloc": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_size_t, c_void_p, c_uint64, c_uint32, c_uint32,
                                        c_double, c_double, c_int, c_int, c_void_p]),
+    "hm_noalloc_prepare": (None, []),
     "hm_fp64_peak": (None, [c_double, _PD, _PD]),
     "hm_release_cached_memory": (None, []),
     "hm_set_profiling": (None, [c_int]),

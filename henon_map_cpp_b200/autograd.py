@@ -115,8 +115,9 @@ def per_particle(x0, px0, y0, py0, theta, n_turns: int, barrier: float = 10.0,
                  checkpoint_every: int = 100, arith: str = "exact", mode: str = "adjoint",
                  reverse: str = "inverse"):
     """Per-particle values without autograd: dict with loss, survived, steps
-    and (mode "adjoint") grad_ic [4, n], grad_theta [4, n] or (mode
-    "tangent") grad_ic from forward-mode tangent-map propagation."""
+    and grad_ic [4, n], grad_theta [4, n]: by the reverse sweep (mode
+    "adjoint") or by forward-mode propagation of the tangent map and of the
+    state's theta derivatives (mode "tangent")."""
     m = {"adjoint": _REVERSE[reverse], "tangent": 1, "loss": 2}[mode]
     a = C.ARITH_FAST if arith == "fast" else C.ARITH_EXACT
     loss, surv, steps, g_ic, g_th = _run(x0, px0, y0, py0, theta, int(n_turns), float(barrier),
@@ -124,6 +125,6 @@ def per_particle(x0, px0, y0, py0, theta, n_turns: int, barrier: float = 10.0,
     out = {"loss": loss, "survived": surv.bool(), "steps": steps}
     if m != 2:
         out["grad_ic"] = g_ic
-    if m in (0, 3):
+    if m != 2:
         out["grad_theta"] = g_th
     return out

@@ -50,8 +50,9 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, c
         t->adjoint_cached = true;
         t->adjoint_has_ripple = false;
     }
-    if (reverse && !t->adjoint_has_ripple) {
-        // Only the reverse sweeps need d omega / d theta (and an "sps" or
+    const bool need_ripple = reverse || (mode == 1 && grad_theta != nullptr);
+    if (need_ripple && !t->adjoint_has_ripple) {
+        // Only the theta gradients need d omega / d theta (and an "sps" or
         // "basic" modulation).
         std::vector<double> ripple;
         HM_TRY(hm::modulation_ripple(t->kind, n_turns, t->omega_0, t->offset, ripple));
@@ -85,7 +86,7 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, c
     a.survived = survived;
     a.steps = steps;
     a.g_ic = grad_ic;
-    a.g_th = grad_theta;
+    a.g_th = mode == 2 ? nullptr : grad_theta;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     HM_CUDA_TRY(hm::launch_adjoint(a, mode, s));
     HM_CUDA_TRY(cudaStreamSynchronize(s));

@@ -389,34 +389,41 @@ __global__ void __launch_bounds__(kThreads) adjoint_inverse_kernel(const Adjoint
 
 // Forward mode: loss and, with TANGENT, g = sum_k w_k M_{k+1}^T grad A(x_{k+1})
 // with M_{k+1} = DF_k ... DF_0 (DF_k = tangent_matrix at x_k, table[k]).
+// When a.g_th is given it also carries P_{k+1} = d x_{k+1} / d theta
+// (4 x 4: state by theta = (omega_x0, omega_y0, epsilon, mu)),
+//     P_{k+1} = DF_k P_k + E_k,
+// E_k the explicit derivative of turn k: the rotation by omega(k) gives
+// d(x', px')/d omega = (px', -x') (and likewise in y), with
+// d omega(k)/d omega0 = 1 + epsilon S_k and d omega(k)/d epsilon = omega0 S_k;
+// the octupole gives d(px1, py1)/d mu = (x^3 - 3 x y^2, y^3 - 3 x^2 y) at the
+// turn's entry point, rotated with the turn.  Then
+//     dL/dtheta_j = sum_k w_k grad A(x_{k+1}) . P_{k+1}[:, j],
+// an independent check of the reverse sweep's theta gradient.
 template <int ARITH, bool OCT, bool TANGENT>
 __global__ void __launch_bounds__(128) forward_loss_kernel(const AdjointArgs a) {
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const size_t n = a.n;
+    const bool theta = TANGENT && a.g_th != nullptr;
     dev::Particle s = dev::make_particle(a.x0[i], a.px0[i], a.y0[i], a.py0[i]);
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     bool alive = !dev::is_lost(s.x, s.px, s.y, s.py);
     double M[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    double P[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     double g[4] = {0, 0, 0, 0};
+    double gt[4] = {0, 0, 0, 0};
     double loss = 0.0;
     uint32_t k = 0;
     for (; alive && k < a.n_turns; ++k) {
         const dev::Turn t = dev::load_turn(a.table, k);
+        double df[16];
+        double u = 0.0, v = 0.0;
         if (TANGENT) {
-            double df[16], out[16];
             dev::tangent_matrix_exact(s.x, s.y, t, a.mu, df);
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc = fma(df[r * 4 + q], M[q * 4 + c], acc);
-                    out[r * 4 + c] = acc;
-                }
-#pragma unroll
-            for (int q = 0; q < 16; ++q) M[q] = out[q];
+            if (theta) {
+                u = s.x * fma(-3.0, s.yy, s.xx);  // x^3 - 3 x y^2
+                v = s.y * fma(-3.0, s.xx, s.yy);  // y^3 - 3 x^2 y
+            }
         }
         bool in;
         const double r = fwd<ARITH, OCT>(s, t, a.mu, bar, in);
@@ -426,11 +433,55 @@ __global__ void __launch_bounds__(128) forward_loss_kernel(const AdjointArgs a) 
         }
         loss = fma(a.w[k], r, loss);
         if (TANGENT) {
+            double out[16];
+#pragma unroll
+            for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc = fma(df[rr * 4 + q], M[q * 4 + c], acc);
+                    out[rr * 4 + c] = acc;
+                }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) M[q] = out[q];
             const double w2 = 2.0 * a.w[k];
-            const double v[4] = {w2 * s.x, w2 * s.px, w2 * s.y, w2 * s.py};
+            const double vv[4] = {w2 * s.x, w2 * s.px, w2 * s.y, w2 * s.py};
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                g[c] = fma(M[c], v[0], fma(M[4 + c], v[1], fma(M[8 + c], v[2], fma(M[12 + c], v[3], g[c]))));
+                g[c] = fma(M[c], vv[0], fma(M[4 + c], vv[1], fma(M[8 + c], vv[2], fma(M[12 + c], vv[3], g[c]))));
+            if (theta) {
+#pragma unroll
+                for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        double acc = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc = fma(df[rr * 4 + q], P[q * 4 + c], acc);
+                        out[rr * 4 + c] = acc;
+                    }
+                const double Sk = a.S[k];
+                const double f0 = fma(a.epsilon, Sk, 1.0);  // d omega(k) / d omega0
+                const double ex = a.omega_x0 * Sk, ey = a.omega_y0 * Sk;  // d omega / d eps
+                // columns: 0 omega_x0, 1 omega_y0, 2 epsilon, 3 mu
+                out[0 * 4 + 0] = fma(s.px, f0, out[0 * 4 + 0]);
+                out[1 * 4 + 0] = fma(-s.x, f0, out[1 * 4 + 0]);
+                out[2 * 4 + 1] = fma(s.py, f0, out[2 * 4 + 1]);
+                out[3 * 4 + 1] = fma(-s.y, f0, out[3 * 4 + 1]);
+                out[0 * 4 + 2] = fma(s.px, ex, out[0 * 4 + 2]);
+                out[1 * 4 + 2] = fma(-s.x, ex, out[1 * 4 + 2]);
+                out[2 * 4 + 2] = fma(s.py, ey, out[2 * 4 + 2]);
+                out[3 * 4 + 2] = fma(-s.y, ey, out[3 * 4 + 2]);
+                out[0 * 4 + 3] = fma(t.sx, u, out[0 * 4 + 3]);
+                out[1 * 4 + 3] = fma(t.cx, u, out[1 * 4 + 3]);
+                out[2 * 4 + 3] = fma(t.sy, v, out[2 * 4 + 3]);
+                out[3 * 4 + 3] = fma(t.cy, v, out[3 * 4 + 3]);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) P[q] = out[q];
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    gt[c] = fma(P[c], vv[0], fma(P[4 + c], vv[1], fma(P[8 + c], vv[2], fma(P[12 + c], vv[3], gt[c]))));
+            }
         }
     }
     a.steps[i] = alive ? a.n_turns : k;
@@ -439,6 +490,10 @@ __global__ void __launch_bounds__(128) forward_loss_kernel(const AdjointArgs a) 
     if (TANGENT) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) a.g_ic[size_t(c) * n + i] = alive ? g[c] : 0.0;
+        if (theta) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) a.g_th[size_t(c) * n + i] = alive ? gt[c] : 0.0;
+        }
     }
 }
 

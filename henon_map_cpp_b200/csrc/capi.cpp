@@ -957,9 +957,17 @@ hm_status hm_fp64_peak(double seconds_target, double *tflops, double *ms) {
     HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     hm::DeviceBuffer sink;
     HM_TRY(sink.alloc(size_t(sms) * 64 * sizeof(double)));
-    cudaEvent_t a, b;
-    HM_CUDA_TRY(cudaEventCreate(&a));
-    HM_CUDA_TRY(cudaEventCreate(&b));
+    // Destroyed on every return path, the early error returns included.
+    struct EventPair {
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~EventPair() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } ev;
+    HM_CUDA_TRY(cudaEventCreate(&ev.a));
+    HM_CUDA_TRY(cudaEventCreate(&ev.b));
+    cudaEvent_t a = ev.a, b = ev.b;
     const int blocks = sms * 8, threads = 256;
     int iters = 256;
     double flops = 0.0;
@@ -977,8 +985,6 @@ hm_status hm_fp64_peak(double seconds_target, double *tflops, double *ms) {
             iters = int(std::min(double(iters) * std::min(scale * 1.1, 8.0), 1e8));
         }
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     *tflops = flops / (double(elapsed) * 1e-3) / 1e12;
     if (ms) *ms = elapsed;
     return ok();

@@ -11,9 +11,13 @@
 //
 // The array is a file-scope __device__ variable of HM_NOALLOC_MAX_PARTICLES
 // particles' worth of scratch (about 9 MiB); every GPU that loads the
-// library holds it until the process exits.  Its name in host code is only
-// a host-side stand-in, so the device address is fetched once per device
-// with cudaGetSymbolAddress (with that device current) and cached.
+// library's device code holds it until the process exits.  Its name in host
+// code is only a host-side stand-in, so the device address is fetched once
+// per device with cudaGetSymbolAddress (with that device current) and
+// cached.  With CUDA's lazy module loading that first lookup is also what
+// loads the device code, and so what takes the array's device memory: a
+// caller that reserves all device memory must do the set-up first
+// (hm_noalloc_prepare, or one early call).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -65,10 +69,25 @@ extern "C" hm_status hm_track_device_noalloc(double *x, double *px, double *y, d
                         "hm_track_device_noalloc: n exceeds the fixed scratch of " +
                             std::to_string(HM_NOALLOC_MAX_PARTICLES) +
                             " particles; use hm_track_device with a caller workspace");
+    // The scratch address is the current device's: a stream of another
+    // device would run the kernels there against this device's array.
+    int cur = 0, sdev = 0;
+    HM_CUDA_TRY(cudaGetDevice(&cur));
+    HM_CUDA_TRY(cudaStreamGetDevice(static_cast<cudaStream_t>(stream), &sdev));
+    if (sdev != cur)
+        return hm::fail(HM_ERR_INVALID_ARG,
+                        "hm_track_device_noalloc: the stream belongs to another device than the "
+                        "current one");
     void *scratch = nullptr;
     HM_TRY(hm::scratch_address(&scratch));
     uint32_t done = 0;
     return hm::track_driver(x, px, y, py, steps, n, tables, table_len, start_step, n_turns, mu,
                             barrier, inverse != 0, arith, scratch,
                             static_cast<cudaStream_t>(stream), &done);
+}
+
+extern "C" hm_status hm_noalloc_prepare(void) {
+    void *scratch = nullptr;
+    HM_TRY(hm::scratch_address(&scratch));
+    return hm::ok();
 }

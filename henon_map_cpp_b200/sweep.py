@@ -66,10 +66,62 @@ def sweep_sets(omega_pairs, epsilons, mus, n_particles: int, n_turns: int,
             for (wx, wy) in omega_pairs for e in epsilons for m in mus]
 
 
+def shard_sets(sets, coords, rank: int, world: int):
+    """This rank's share of a sweep: the set indices that longest-processing-
+    time assignment (sharding.assign_sets, on particles x turns) gives it,
+    those sets, and their points cut out of the concatenated coords.  This
+    replaces the reference's one-GPU-per-job HTCondor submission
+    (htcondor_jobs/htcondor_gpu.sub, run_sim.py:41-74) with one batch per
+    rank."""
+    from .sharding import assign_sets
+
+    offsets = np.concatenate([[0], np.cumsum([int(s["n_particles"]) for s in sets])])
+    mine = assign_sets(sets, world)[rank] if sets else []
+    sub = [sets[k] for k in mine]
+    sub_coords = tuple(
+        np.concatenate([np.asarray(c)[offsets[k]:offsets[k + 1]] for k in mine])
+        if mine else np.zeros(0) for c in coords)
+    return mine, sub, sub_coords
+
+
 def run_sweep(sets, coords, arith: int = C.ARITH_EXACT, per_thread: int = 1,
-              chunk0: int = 512, chunk_max: int = 4096, use_graph: bool = True):
-    """Tracks every set to its budget in one batch; returns a list with one
-    dict per set: x, px, y, py (final) and steps (survival turns)."""
+              chunk0: int = 512, chunk_max: int = 4096, use_graph: bool = True,
+              distributed: bool | None = None, group=None):
+    """Tracks every set to its budget; returns a list with one dict per set:
+    x, px, y, py (final) and steps (survival turns).
+
+    With a torch.distributed process group (distributed=None: whenever one is
+    initialised with more than one rank), each rank tracks the sets that
+    shard_sets assigns it as one batch on its own GPU -- no exchange during
+    tracking -- and the per-set results are then gathered so that every
+    rank returns all of them."""
+    if distributed is None:
+        try:
+            import torch.distributed as dist
+
+            distributed = dist.is_available() and dist.is_initialized() and \
+                dist.get_world_size(group) > 1
+        except ImportError:
+            distributed = False
+    if not distributed:
+        return _local_sweep(sets, coords, arith, per_thread, chunk0, chunk_max, use_graph)
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    mine, sub, sub_coords = shard_sets(sets, coords, rank, world)
+    local = _local_sweep(sub, sub_coords, arith, per_thread, chunk0, chunk_max,
+                         use_graph) if sub else []
+    parts = [None] * world
+    dist.all_gather_object(parts, list(zip(mine, local)), group=group)
+    out = [None] * len(sets)
+    for part in parts:
+        for k, r in part:
+            out[k] = r
+    return out
+
+
+def _local_sweep(sets, coords, arith, per_thread, chunk0, chunk_max, use_graph):
+    """Every set in one batch on the current device."""
     b = C.Batch(sets)
     b.configure(arith, per_thread, chunk0, chunk_max)
     b.load(*coords)
@@ -123,7 +175,9 @@ def run_jobs(jobs, num_points: int = 100, num_iterations: int = 100_000, out_dir
     """Every job of the list in one batch: SPS modulation, barrier 10, each on
     its own grid (run_sim.py:40-47).  Returns the survival turns of each job;
     with out_dir, also writes one file per job holding `steps`: HDF5 as the
-    reference does when h5py is importable, else .npz."""
+    reference does when h5py is importable, else .npz.  Under a
+    torch.distributed process group the jobs are spread over the ranks
+    (run_sweep) and rank 0 writes every file."""
     import os
 
     sets, pts = [], []
@@ -136,7 +190,7 @@ def run_jobs(jobs, num_points: int = 100, num_iterations: int = 100_000, out_dir
         tuple(np.zeros(0) for _ in range(4))
     results = run_sweep(sets, coords, arith=arith) if sets else []
     steps = [r["steps"] for r in results]
-    if out_dir is not None:
+    if out_dir is not None and _rank() == 0:
         os.makedirs(out_dir, exist_ok=True)
         try:
             import h5py  # noqa: PLC0415
@@ -150,6 +204,15 @@ def run_jobs(jobs, num_points: int = 100, num_iterations: int = 100_000, out_dir
             else:
                 np.savez(base + ".npz", steps=st)
     return steps
+
+
+def _rank() -> int:
+    try:
+        import torch.distributed as dist
+
+        return dist.get_rank() if dist.is_available() and dist.is_initialized() else 0
+    except ImportError:
+        return 0
 
 
 def main(argv=None) -> None:

@@ -112,7 +112,10 @@ hm_status hm_get_track_config(int *threads, int *per_thread,
  * stage_turns is 0 or a power of two in [16, 512] (default 256); runs of
  * one chunk use direct reads.  Process-wide; results do not depend on it.
  * A staged copy that does not land within its bounded wait makes the call
- * return HM_ERR_TIMEOUT. */
+ * return HM_ERR_TIMEOUT.  After HM_ERR_TIMEOUT the particles' coordinates
+ * and steps are unspecified (the chunk that gave up may have moved some of
+ * them, and its survivors may still be in the scratch lists), and
+ * global_steps is left unchanged: reset the particles before reusing them. */
 hm_status hm_set_track_staging(uint32_t stage_turns);
 hm_status hm_get_track_staging(uint32_t *stage_turns);
 
@@ -490,8 +493,9 @@ hm_status hm_storage_tunes(const hm_storage *s, const uint32_t *from,
  * for bit); mode 3 instead rebuilds them backwards with the map's exact
  * inverse from the state at the segment's end (no per-turn memory traffic;
  * reconstruction error bounded to one segment).  mode 1 gives grad_ic by
- * forward-mode tangent-map propagation (an independent J^T v), mode 2 the
- * loss only.
+ * forward-mode tangent-map propagation (an independent J^T v) and, when
+ * grad_theta is not NULL, grad_theta by forward propagation of the state's
+ * derivatives with respect to theta alongside it; mode 2 the loss only.
  * Derivatives need an "sps" or "basic" modulation.  Synchronous. */
 size_t hm_adjoint_workspace_bytes(size_t n, uint32_t n_turns,
                                   uint32_t checkpoint_every);
@@ -511,9 +515,15 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0,
  * (room for HM_NOALLOC_MAX_PARTICLES particles, about 9 MiB, held by every
  * GPU that loads the library until the process exits); n above that limit
  * is rejected with HM_ERR_INVALID_ARG.  The first call on each device looks
- * up the array's device address (cudaGetSymbolAddress), so make that first
- * call before any stream capture.  All calls on a device share the array:
- * calls that overlap on the GPU race.  Synchronous. */
+ * up the array's device address (cudaGetSymbolAddress); that lookup can
+ * load the library's device code onto the device, which takes device
+ * memory (the array itself among it), so make that first call -- or
+ * hm_noalloc_prepare -- before the caller reserves its device memory and
+ * before any stream capture.  The current device must own `stream` and the
+ * arrays; a stream of another device is rejected with HM_ERR_INVALID_ARG.
+ * All calls on a device share the array: calls that overlap on the GPU
+ * race.  Particle state after HM_ERR_TIMEOUT is as for hm_track_device.
+ * Synchronous. */
 #define HM_NOALLOC_MAX_PARTICLES 131072u
 hm_status hm_track_device_noalloc(double *x, double *px, double *y, double *py,
                                   uint32_t *steps, size_t n,
@@ -521,6 +531,12 @@ hm_status hm_track_device_noalloc(double *x, double *px, double *y, double *py,
                                   uint32_t start_step, uint32_t n_turns,
                                   double mu, double barrier, int inverse,
                                   hm_arith arith, void *stream);
+/* No counterpart in the reference.  The set-up of hm_track_device_noalloc
+ * for the current device, done ahead of time: it looks up the scratch
+ * array's device address, loading the library's device code if it is not
+ * loaded yet.  Call it once per device at start-up, before reserving device
+ * memory; later calls return at once. */
+hm_status hm_noalloc_prepare(void);
 
 /* ---- device memory ----------------------------------------------------- */
 

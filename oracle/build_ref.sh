@@ -10,8 +10,10 @@
 #              reference GPU path does the same arithmetic as its CPU path
 #   default  : CUDA code built as shipped (nvcc's default --fmad=true)
 # Host code: g++ -O3 without -march (plain SSE2 binary64, no FMA).
+#
+# REF must name the reference checkout (its src/ directory is compiled).
 set -euo pipefail
-REF=${REF:-/root/reference}
+: "${REF:?set REF to the reference checkout (the directory holding src/henon.cu)}"
 HERE=$(cd "$(dirname "$0")" && pwd)
 CUDA=${CUDA_HOME:-/usr/local/cuda}
 PY=${PYTHON:-python3}

@@ -244,9 +244,12 @@ def reference_track_subprocess(variant: str, x, px, y, py, n_turns: int, tunes, 
         return d["x"], d["px"], d["y"], d["py"], d["steps"].astype(np.uint32)
 
 
-def build_reference() -> bool:
-    """Runs oracle/build_ref.sh when the reference sources are present."""
-    if not Path(os.environ.get("REF", "/root/reference"), "src").exists():
+def build_reference(ref: str | os.PathLike | None = None) -> bool:
+    """Runs oracle/build_ref.sh on the reference checkout `ref` (default: the
+    REF environment variable) when its sources are present."""
+    ref = ref if ref is not None else os.environ.get("REF")
+    if not ref or not Path(ref, "src").exists():
         return False
-    subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True)
+    subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True,
+                   env={**os.environ, "REF": str(ref)})
     return True

@@ -139,3 +139,49 @@ def test_autograd_function(gpu):
     with torch.no_grad():
         l2 = AG.orbit_loss(*[p.detach() for p in pts], th.detach(), n_turns)
     torch.testing.assert_close(l2, loss.detach(), rtol=0, atol=0)
+
+
+def _rel(a, t):
+    """Per particle: max over components of |a - t| / max over components of |t|."""
+    return np.max(np.abs(a - t), axis=0) / np.max(np.abs(t), axis=0)
+
+
+def test_adjoint_vs_forward_tangent_c5(gpu):
+    # The adjoint configuration itself: 65,536 particles, x0, y0 ~ U[0, 0.3],
+    # px0, py0 ~ N(0, 0.01^2), eps 16, mu 0.1, N = 10^4, checkpoints every
+    # 100.  The reverse sweep's gradients with respect to the initial
+    # conditions AND theta = (omega_x0, omega_y0, eps, mu) against forward-
+    # mode propagation of the tangent map and of d x / d theta.
+    #
+    # Conditioning criterion.  Both sides sum N terms w_k grad A . (d x_k /
+    # d input); their rounding errors grow like the tangent map itself, so
+    # the relative difference of particle i is bounded by c u kappa_i with
+    # kappa_i = max_c |dL_i/d x0_c| (the size of the propagated tangent map
+    # seen through the loss) and u = 2^-53.  Required:
+    #   * every particle with kappa_i <= 1e3 (well conditioned): within 1e-10
+    #     relative, for grad_ic and for each component of grad_theta;
+    #   * every particle: relative difference <= 1e-13 * max(1, kappa_i);
+    #   * the configuration's well-conditioned particles are the majority.
+    n_turns = 10_000
+    pts = c5_points(65_536, seed=5)
+    th = torch.tensor(THETA, dtype=torch.float64)
+    adj = AG.per_particle(*pts, th, n_turns, checkpoint_every=100, reverse="inverse")
+    tan = AG.per_particle(*pts, th, n_turns, mode="tangent")
+    surv = adj["survived"].cpu().numpy()
+    np.testing.assert_array_equal(surv, tan["survived"].cpu().numpy())
+    assert surv.sum() > 60_000
+    a_ic, t_ic = adj["grad_ic"].cpu().numpy()[:, surv], tan["grad_ic"].cpu().numpy()[:, surv]
+    a_th, t_th = adj["grad_theta"].cpu().numpy()[:, surv], tan["grad_theta"].cpu().numpy()[:, surv]
+    kappa = np.max(np.abs(t_ic), axis=0)
+    well = kappa <= 1e3
+    rel_ic = _rel(a_ic, t_ic)
+    rel_th = np.abs(a_th - t_th) / np.abs(t_th)
+    stats = (f"well-conditioned {well.mean():.4f}; rel_ic max (well) {rel_ic[well].max():.2e}; "
+             f"rel_theta max (well) {rel_th[:, well].max(axis=1)}; kappa max {kappa.max():.2e}; "
+             f"max rel/kappa {np.max(np.maximum(rel_ic, rel_th.max(axis=0)) / np.maximum(1, kappa)):.2e}")
+    print("\n" + stats)
+    assert well.mean() >= 0.5, stats
+    assert np.all(rel_ic[well] < 1e-10), stats
+    assert np.all(rel_th[:, well] < 1e-10), stats
+    assert np.all(rel_ic <= 1e-13 * np.maximum(1.0, kappa)), stats
+    assert np.all(rel_th <= 1e-13 * np.maximum(1.0, kappa)), stats

@@ -48,3 +48,41 @@ def test_workload_config_names_the_scan():
     cfg = bench.workload_config(args, 4)
     assert cfg["particles_per_gpu"] == 1024 * 1024 and cfg["turns"] == 100_000
     assert cfg["parallelism"] == "particle shards x4"
+
+
+def _bench_json(cmd, env=None):
+    import json
+    import os
+    import subprocess
+
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=240,
+                         env={**os.environ, **(env or {})}, cwd=str(Path(bench.__file__).parent))
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    return json.loads(lines[0])
+
+
+def test_gpus_flag_starts_that_many_ranks():
+    # Without torchrun's environment, --gpus 2 re-executes bench.py under
+    # torch.distributed.run with two ranks; with no GPU they join over gloo.
+    line = _bench_json([sys.executable, "bench.py", "--gpus", "2", "--launch-check"],
+                       env={"CUDA_VISIBLE_DEVICES": ""})
+    assert line["n_gpus"] == 2 and line["backend"] == "gloo"
+    assert sorted(r["rank"] for r in line["ranks"]) == [0, 1]
+
+
+def test_world_size_must_match_gpus(monkeypatch):
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    with pytest.raises(SystemExit, match="WORLD_SIZE=2"):
+        bench.check_world(type("A", (), {"gpus": 4})())
+
+
+def test_cpu_sample_is_fixed():
+    # Both the reference arm and the GPU arm's cpu_baseline leg time the
+    # same fixed stride of the grid.
+    import inspect
+
+    assert bench.CPU_STRIDE == 16
+    sig = inspect.signature(bench.reference_cpu_sample)
+    assert sig.parameters["stride"].default == bench.CPU_STRIDE

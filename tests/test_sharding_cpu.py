@@ -85,3 +85,72 @@ def test_collectives_two_gloo_ranks():
         assert mean == pytest.approx(total / 3)
         assert gmean == pytest.approx([(1 + 2) / 3] * 4)
         assert steps == [0, 1, 2, 10, 11, 12, 13]
+
+
+def test_shard_sets_cut_the_concatenated_points():
+    sets, coords = sweep.heterogeneous_sets(seed=7, n_sets=9, n_range=(3, 40),
+                                            turn_range=(10, 1000))
+    offsets = np.concatenate([[0], np.cumsum([s["n_particles"] for s in sets])])
+    seen = []
+    for world in (1, 2, 3):
+        seen = []
+        for rank in range(world):
+            mine, sub, sub_coords = sweep.shard_sets(sets, coords, rank, world)
+            seen += mine
+            assert [sets[k] for k in mine] == sub
+            want = [np.concatenate([c[offsets[k]:offsets[k + 1]] for k in mine]) for c in coords]
+            for a, b in zip(sub_coords, want):
+                np.testing.assert_array_equal(a, b)
+        assert sorted(seen) == list(range(len(sets)))
+
+
+def _sweep_worker(rank, world, port, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sets, coords = sweep.heterogeneous_sets(seed=7, n_sets=9, n_range=(3, 40),
+                                                turn_range=(10, 1000))
+        ran = []
+
+        def fake_local(sub, sub_coords, *args):
+            # Stands in for the device batch: steps = the set's turn budget
+            # minus its first x coordinate's rank in the set, so results are
+            # tied to both the set and its points.
+            ran.extend(s["n_turns"] for s in sub)
+            out_l, o = [], 0
+            for s in sub:
+                n = s["n_particles"]
+                out_l.append({"steps": np.full(n, s["n_turns"], np.uint32),
+                              "x": np.asarray(sub_coords[0][o:o + n])})
+                o += n
+            return out_l
+
+        sweep._local_sweep = fake_local
+        res = sweep.run_sweep(sets, coords)
+        out[rank] = ([r["steps"].tolist() for r in res], [r["x"].tolist() for r in res],
+                     sorted(ran))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sweep_spreads_sets_over_two_gloo_ranks():
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_sweep_worker, args=(2, port, out), nprocs=2, join=True)
+        res = dict(out)
+    sets, coords = sweep.heterogeneous_sets(seed=7, n_sets=9, n_range=(3, 40),
+                                            turn_range=(10, 1000))
+    offsets = np.concatenate([[0], np.cumsum([s["n_particles"] for s in sets])])
+    parts = S.assign_sets(sets, 2)
+    for r in range(2):
+        steps, xs, ran = res[r]
+        # each rank tracked only its own sets ...
+        assert ran == sorted(sets[k]["n_turns"] for k in parts[r])
+        # ... and every rank returns every set's result, in set order
+        for k, s in enumerate(sets):
+            assert steps[k] == [s["n_turns"]] * s["n_particles"]
+            np.testing.assert_array_equal(xs[k], coords[0][offsets[k]:offsets[k + 1]])

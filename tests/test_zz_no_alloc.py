@@ -7,8 +7,9 @@ synchronisation).  This entry point keeps its scratch in a fixed device
 array built into the library instead of a caller workspace.  The test runs
 it twice in a row through the C ABI and checks each result bit for bit
 against hm_track_device (the allocating entry point, given a workspace) on
-the same inputs -- exact arithmetic, so the tolerance is zero -- and that a
-size above the fixed limit is refused.  The file name sorts last so that
+the same inputs -- exact arithmetic, so the tolerance is zero -- that the
+device's free memory is the same before and after the second call (nothing
+was allocated), and that a size above the fixed limit is refused.  The file name sorts last so that
 pytest collects it after every other test.
 """
 from __future__ import annotations
@@ -44,14 +45,23 @@ def test_noalloc_matches_allocating_entry_point_twice(gpu):
     trackers = [C.Tracker(n_turns, TUNES[0], TUNES[1], "sps", NAN, eps, 0) for eps in (64.0, 16.0)]
     ws = torch.empty(C.load().hm_track_workspace_bytes(n), dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
+    C.call("hm_noalloc_prepare")
     for call, (tr, mu) in enumerate(zip(trackers, (0.2, 0.0))):
         ref_c, ref_s = _device_state(torch, x, px, y, py)
         C.call("hm_track_device", *[c.data_ptr() for c in ref_c], ref_s.data_ptr(), n,
                tr.device_tables(), n_turns, 0, n_turns, mu, 10.0, 0, C.ARITH_EXACT,
                ws.data_ptr(), stream)
         got_c, got_s = _device_state(torch, x, px, y, py)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         C.call("hm_track_device_noalloc", *[c.data_ptr() for c in got_c], got_s.data_ptr(), n,
                tr.device_tables(), n_turns, 0, n_turns, mu, 10.0, 0, C.ARITH_EXACT, stream)
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        if call == 1:
+            # The set-up was done by hm_noalloc_prepare and the first call:
+            # the second takes no device memory at all.
+            assert free_after == free_before, (free_before, free_after)
         want, want_steps = _host(torch, ref_c, ref_s)
         have, have_steps = _host(torch, got_c, got_s)
         np.testing.assert_array_equal(have_steps, want_steps, err_msg=f"call {call}")
