@@ -553,11 +553,14 @@ def bench_kicks(C, turns=10_000, side=512):
             "timing": "wall clock around one hm_track call"}
 
 
-def bench_ghosts(C, turns=1000, side=256, every=10):
+def bench_ghosts(C, turns=1000, side=256, every=10, fused_turns=20_000):
     """The displacement (ghost) Lyapunov loop of tests/test_new_standard.ipynb
-    through the drop-in facade: 256x256 base particles on [0, 0.5]^2 with x
-    and y ghosts at 1e-10, tracked `every` turns at a time, displacement read
-    and ghosts renormalised after each step (eps 64, mu 0)."""
+    on 256x256 base particles on [0, 0.5]^2 with x and y ghosts at 1e-10
+    (eps 64, mu 0), renormalised every 10 turns: as the notebook runs it
+    through the drop-in facade (track + displacement read + renormalize per
+    step, `turns` turns), and fused (track_ghost_lyapunov, `fused_turns`
+    turns, the same steps); the fused result is checked against the loop on
+    the loop's horizon."""
     import torch
 
     import henon_map_cpp_b200 as hm
@@ -566,25 +569,55 @@ def bench_ghosts(C, turns=1000, side=256, every=10):
     xx, yy = np.meshgrid(v, v)
     x, y = xx.ravel(), yy.ravel()
     z = np.zeros_like(x)
-    p = hm.particles(x, z, y, z)
-    p.add_ghost(1e-10, "x")
-    p.add_ghost(1e-10, "y")
-    t = hm.henon_tracker(turns + every, 0.168, 0.201, "sps", np.nan, 64.0, 0)
-    lyap = np.zeros(2 * x.size)
+
+    def make(n_turns):
+        p = hm.particles(x, z, y, z)
+        p.add_ghost(1e-10, "x")
+        p.add_ghost(1e-10, "y")
+        t = hm.henon_tracker(n_turns + every, 0.168, 0.201, "sps", np.nan, 64.0, 0)
+        return p, t
+
+    p, t = make(turns)
+    lyap = np.zeros((x.size, 2))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(turns // every):
         t.track(p, every, 0.0)
-        lyap += np.log(np.asarray(p.get_displacement_module()).ravel() / 1e-10)
+        lyap += np.log(np.asarray(p.get_displacement_module()).reshape(x.size, 2) / 1e-10)
         p.renormalize(1e-10)
     torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
+    loop_s = time.perf_counter() - t0
+
+    q, tq = make(turns)
+    fused_lyap = tq.track_ghost_lyapunov(q, turns // every, every, 0.0, 1e-10)
+    same_state = all(np.array_equal(np.asarray(getattr(p, g)()), np.asarray(getattr(q, g)()),
+                                    equal_nan=True)
+                     for g in ("get_x", "get_px", "get_y", "get_py", "get_steps"))
+    m = np.isfinite(lyap)
+    lyap_rel = float(np.max(np.abs(fused_lyap[m] - lyap[m]) / np.maximum(np.abs(lyap[m]), 1e-300))) \
+        if m.any() else 0.0
+
+    q, tq = make(fused_turns)
+    tq.track_ghost_lyapunov(q, 10, every, 0.0, 1e-10)  # warm-up
+    q, tq = make(fused_turns)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tq.track_ghost_lyapunov(q, fused_turns // every, every, 0.0, 1e-10)
+    torch.cuda.synchronize()
+    fused_s = time.perf_counter() - t0
     n_all = 3 * x.size
     return {"workload": f"{side}x{side} base particles + x and y ghosts at 1e-10, eps 64, mu 0, "
-                        f"{turns} turns, renormalised every {every}",
-            "seconds": dt, "particle_turns_per_s": n_all * turns / dt,
-            "steps_per_s": (turns // every) / dt,
-            "timing": "wall clock; each step is track + displacement read + renormalize"}
+                        f"renormalised every {every}",
+            "loop_turns": turns, "loop_seconds": loop_s,
+            "loop_particle_turns_per_s": n_all * turns / loop_s,
+            "loop_steps_per_s": (turns // every) / loop_s,
+            "fused_turns": fused_turns, "fused_seconds": fused_s,
+            "fused_particle_turns_per_s": n_all * fused_turns / fused_s,
+            "fused_over_loop": (n_all * fused_turns / fused_s) / (n_all * turns / loop_s),
+            "fused_state_bit_equal_to_loop": bool(same_state),
+            "fused_lyap_max_rel_diff": lyap_rel,
+            "timing": "wall clock; each loop step is track + displacement read + renormalize; "
+                      "the fused call is one synchronous call"}
 
 
 # ---- reference arm ---------------------------------------------------------------

@@ -378,6 +378,19 @@ class henon_tracker:
     def get_tangent_matrix(self, particles, mu, reverse=False):
         return self.tracker.get_tangent_matrix(particles.particles, mu, reverse)
 
+    def track_ghost_lyapunov(self, particles, n_steps, every, mu, module, barrier=10.0):
+        """The displacement Lyapunov loop of the reference's notebooks,
+
+            for _ in range(n_steps):
+                tracker.track(particles, every, mu, barrier)
+                lyap += np.log(particles.get_displacement_module() / module)
+                particles.renormalize(module)
+
+        in fused GPU launches; returns lyap (n_particles x n_ghosts) and
+        leaves the particles as that loop does."""
+        return np.asarray(self.tracker.track_ghost_lyapunov(particles.particles, int(n_steps),
+                                                            int(every), mu, barrier, module))
+
     # ---- additions ---------------------------------------------------------------
     def set_arith(self, mode: str) -> None:
         """'exact' (default; bit-identical to the reference CPU path) or

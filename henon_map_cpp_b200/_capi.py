@@ -98,7 +98,6 @@ _SIGNATURES = {
     "hm_track_device_noalloc": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_size_t, c_void_p, c_uint64, c_uint32, c_uint32,
                                        c_double, c_double, c_int, c_int, c_void_p]),
-    "hm_noalloc_prepare": (None, []),
     "hm_fp64_peak": (None, [c_double, _PD, _PD]),
     "hm_release_cached_memory": (None, []),
     "hm_set_profiling": (None, [c_int]),
@@ -162,6 +161,8 @@ _SIGNATURES = {
     "hm_particles_displacement_module": (None, [c_void_p, _PD]),
     "hm_particles_displacement_direction": (None, [c_void_p, _PD]),
     "hm_tracker_tangent_matrices": (None, [c_void_p, c_void_p, c_double, c_int, _PD]),
+    "hm_track_ghost_lyapunov": (None, [c_void_p, c_void_p, c_uint32, c_uint32, c_double,
+                                       c_double, c_double, _PD]),
     # batched heterogeneous tracking
     "hm_batch_create": (None, [c_size_t, c_void_p, POINTER(c_void_p)]),
     "hm_batch_destroy": (None, [c_void_p]),
@@ -175,8 +176,10 @@ _SIGNATURES = {
     # tunes
     "hm_orbit_tunes": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t,
                               _PU32, _PU32, c_size_t, c_int, _PD]),
-    "hm_tracker_orbit_tunes": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, _PU32,
-                                      _PU32, c_size_t, c_int, _PD, _PD]),
+    "hm_tracker_megno": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double, c_double,
+                                c_int, POINTER(c_uint64), c_size_t, _PD]),
+    "hm_tracker_orbit_tunes": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double,
+                                      c_double, c_int, _PU32, _PU32, c_size_t, c_int, _PD, _PD]),
     "hm_storage_tunes": (None, [c_void_p, _PU32, _PU32, c_size_t, c_int, _PD]),
     "hm_orbit_tunes_host": (None, [_PD, _PD, _PD, _PD, c_size_t, c_size_t, _PU32, _PU32,
                                    c_size_t, c_int, _PD]),
@@ -669,15 +672,17 @@ def _windows(frm, to):
 
 
 def tracker_orbit_tunes(tracker: Tracker, particles: Particles, n_turns: int, mu: float,
-                        barrier: float, frm, to, remove_mean: bool, fft: bool):
+                        barrier: float, frm, to, remove_mean: bool, fft: bool,
+                        kick_module: float = float("nan"), inverse: bool = False):
     """hm_tracker_orbit_tunes: (birkhoff [n][2(W+1)], fft or None)."""
     f, t = _windows(frm, to)
     n = particles.n_total
     b = np.empty((n, 2 * (f.size + 1)))
     ff = np.empty_like(b) if fft else None
     call("hm_tracker_orbit_tunes", tracker.h, particles.h, int(n_turns), float(mu),
-         float(barrier), f.ctypes.data_as(_PU32), t.ctypes.data_as(_PU32), f.size,
-         int(bool(remove_mean)), dptr(b), dptr(ff) if fft else None)
+         float(barrier), float(kick_module), int(bool(inverse)), f.ctypes.data_as(_PU32),
+         t.ctypes.data_as(_PU32), f.size, int(bool(remove_mean)), dptr(b),
+         dptr(ff) if fft else None)
     return b, ff
 
 

@@ -436,6 +436,22 @@ class storage_4d(_CpuClassNotProvided):
             check(s);
         }, "Track particles", py::arg("particles"), py::arg("n_turns"), py::arg("mu"),
            py::arg("barrier") = 100.0, py::arg("kick_module") = NAN, py::arg("inverse") = false)
+        .def("track_ghost_lyapunov", [](Tracker &t, Particles &p, unsigned n_steps,
+                                        unsigned every, double mu, double barrier,
+                                        double module) {
+            auto out = array2(p.n_particles(), p.n_ghosts());
+            hm_status s;
+            double *dst = out.mutable_data();
+            {
+                py::gil_scoped_release nogil;
+                s = hm_track_ghost_lyapunov(t.h, p.h, n_steps, every, mu, barrier, module, dst);
+            }
+            check(s);
+            return out;
+        }, "n_steps x (track `every` turns; sum log(displacement / module); renormalize) "
+           "in fused launches",
+           py::arg("particles"), py::arg("n_steps"), py::arg("every"), py::arg("mu"),
+           py::arg("barrier"), py::arg("module"))
         .def("get_tangent_matrix", [](const Tracker &t, const Particles &p, double mu,
                                       bool reverse) {
             const size_t n = p.n_total();
@@ -464,8 +480,6 @@ class storage_4d(_CpuClassNotProvided):
             // henon_tracker::birkhoff_tunes (src/henon.cu:2890-2967): the
             // window [0, n_turns] is appended to the caller's, then the full
             // orbit; result [n][2 (W + 2)].
-            if (!std::isnan(kick) || inverse)
-                throw std::domain_error("birkhoff_tunes: kicks and inverse tracking are not provided");
             if (from.size() != to.size())
                 throw std::runtime_error("compute_tune: from and to must be of the same size");
             from.push_back(0);
@@ -474,8 +488,9 @@ class storage_4d(_CpuClassNotProvided):
             hm_status s;
             {
                 py::gil_scoped_release nogil;
-                s = hm_tracker_orbit_tunes(t.h, p.h, n_turns, mu, barrier, from.data(), to.data(),
-                                           from.size(), 0, out.mutable_data(), nullptr);
+                s = hm_tracker_orbit_tunes(t.h, p.h, n_turns, mu, barrier, kick, inverse ? 1 : 0,
+                                           from.data(), to.data(), from.size(), 0,
+                                           out.mutable_data(), nullptr);
             }
             check(s);
             return out;
@@ -487,8 +502,6 @@ class storage_4d(_CpuClassNotProvided):
                              std::vector<uint32_t> to) {
             // henon_tracker::all_tunes (src/henon.cu:2969-3078): orbit mean
             // removed, Birkhoff and FFT tunes; ([n][2(W+2)], [n][2(W+2)]).
-            if (!std::isnan(kick) || inverse)
-                throw std::domain_error("all_tunes: kicks and inverse tracking are not provided");
             if (from.size() != to.size())
                 throw std::runtime_error("compute_tune: from and to must be of the same size");
             from.push_back(0);
@@ -498,8 +511,9 @@ class storage_4d(_CpuClassNotProvided):
             hm_status s;
             {
                 py::gil_scoped_release nogil;
-                s = hm_tracker_orbit_tunes(t.h, p.h, n_turns, mu, barrier, from.data(), to.data(),
-                                           from.size(), 1, b.mutable_data(), f.mutable_data());
+                s = hm_tracker_orbit_tunes(t.h, p.h, n_turns, mu, barrier, kick, inverse ? 1 : 0,
+                                           from.data(), to.data(), from.size(), 1,
+                                           b.mutable_data(), f.mutable_data());
             }
             check(s);
             return py::make_tuple(b, f);
@@ -512,30 +526,16 @@ class storage_4d(_CpuClassNotProvided):
             // with the GPU construct's definition (Frobenius norm of the
             // tangent map, src/henon.cu:2253-2284) and the tangent map of each
             // turn; values at the turn counts in turn_samples: [n][samples].
-            if (!std::isnan(kick) || inverse)
-                throw std::domain_error("megno: kicks and inverse tracking are not provided");
             if (samples.empty()) samples.push_back(n_turns);
-            const size_t n = p.n_total();
-            Matrices M(n);
-            Megno g(n);
-            std::vector<double> snap(samples.size() * n, std::numeric_limits<double>::quiet_NaN());
-            hm_indicator_set s{};
-            s.matrix = M.h;
-            s.megno = g.h;
-            s.megno_sample_turns = samples.data();
-            s.n_megno_samples = samples.size();
-            s.megno_samples_out = snap.data();
-            s.jacobian_of_turn = 1;
+            auto out = array2(p.n_total(), samples.size());
+            double *o = out.mutable_data();
             hm_status st;
             {
                 py::gil_scoped_release nogil;
-                st = hm_track_indicators(t.h, p.h, n_turns, mu, barrier, &s);
+                st = hm_tracker_megno(t.h, p.h, n_turns, mu, barrier, kick, inverse ? 1 : 0,
+                                      samples.data(), samples.size(), o);
             }
             check(st);
-            auto out = array2(n, samples.size());
-            double *o = out.mutable_data();
-            for (size_t i = 0; i < n; ++i)
-                for (size_t j = 0; j < samples.size(); ++j) o[i * samples.size() + j] = snap[j * n + i];
             return out;
         }, py::arg("particles"), py::arg("n_turns"), py::arg("mu"), py::arg("barrier") = 100.0,
            py::arg("kick_module") = NAN, py::arg("inverse") = false,

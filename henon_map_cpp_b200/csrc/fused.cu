@@ -36,7 +36,9 @@ using dev::Rn;
 // holds about half of a particle's window accumulators, so the same shared
 // memory holds twice the threads: the loop is a long chain of dependent
 // FP64 operations, and more warps per SM hide its latency.
-template <bool OCT, bool DO_M, bool DO_V, bool DO_T, bool SPLIT>
+// EXT: kicks and backward turns (whole-orbit MEGNO: DO_M alone, the
+// Jacobian of each turn at the point before it).
+template <bool OCT, bool DO_M, bool DO_V, bool DO_T, bool SPLIT, bool EXT = false>
 __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const FusedArgs a) {
     extern __shared__ double smem[];
     const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -108,18 +110,35 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
     uint32_t k = 0;
     for (; k < a.n_turns && warp_live; ++k) {
         double df[16];
+        const bool rev = EXT && a.inverse;
+        const uint32_t tidx = rev ? a.live_step - 1u - k : a.live_step + k;
         // ---- Jacobian of the turn, at the point before it (option) ------------
         if ((do_m || do_v) && a.df_before) {
-            const dev::Turn td = dev::load_turn(a.table, a.live_step + k);
-            dev::tangent_matrix_exact(x, y, td, mu, df);
+            const dev::Turn td = dev::load_turn(a.table, tidx);
+            if (rev) dev::inverse_tangent_matrix_exact(x, px, y, py, td, mu, df);
+            else dev::tangent_matrix_exact(x, y, td, mu, df);
         }
         // ---- track(p, 1) ------------------------------------------------------
         if (alive) {
-            const dev::Turn t = dev::load_turn(a.table, a.live_step + k);
+            const dev::Turn t = dev::load_turn(a.table, tidx);
             dev::Particle q = dev::make_particle(x, px, y, py);
-            dev::turn<HM_ARITH_EXACT, OCT, false>(q, t, mu);
+            if (EXT) {
+                // kicks as hm_track: before the forward turn, subtracted
+                // after the backward one, keyed by the particle's index
+                const bool kick = !isnan(a.kick_module);
+                if (kick && !rev)
+                    dev::apply_kick<false>(q, dev::kick_direction(a.kick_seed, ii, tidx),
+                                           a.kick_module);
+                if (rev) dev::turn<HM_ARITH_EXACT, OCT, true>(q, t, mu);
+                else dev::turn<HM_ARITH_EXACT, OCT, false>(q, t, mu);
+                if (kick && rev)
+                    dev::apply_kick<true>(q, dev::kick_direction(a.kick_seed, ii, tidx),
+                                          a.kick_module);
+            } else {
+                dev::turn<HM_ARITH_EXACT, OCT, false>(q, t, mu);
+            }
             if (dev::inside_after_turn<HM_ARITH_EXACT>(q, bar)) {
-                steps += 1u;
+                steps = rev ? steps - 1u : steps + 1u;
                 x = q.x;
                 px = q.px;
                 y = q.y;
@@ -135,17 +154,23 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             dev::tangent_matrix_exact(x, y, td, mu, df);
         }
         if (do_m) {
+            // old_norm is the norm of M: finite exactly when every entry is
+            // (an overflowing sum of finite squares also takes the dense
+            // product, which is then equally right).
             double out[16];
-            dev::matmul4_exact(df, M, out);
+            // (the backward turn's Jacobian has other structural zeros)
+            if (!rev && dev::finite_bits(old_norm)) dev::jacobian_matmul4_exact(df, M, out);
+            else dev::matmul4_exact(df, M, out);
 #pragma unroll
             for (int q = 0; q < 16; ++q) M[q] = out[q];
             const double new_norm = dev::norm_exact<16>(M);
             const double lr = log10(Rn::div(new_norm, old_norm));
             if (a.megno_l1) {
                 const double di = double(a.megno_idx + k);
+                const double inv = Rn::div(1.0, di);  // 1.0/idx, used twice
                 m_l1 = Rn::add(m_l1, Rn::mul(lr, di));
-                m_l2 = Rn::add(m_l2, Rn::mul(Rn::div(1.0, di), m_l1));
-                m_l3 = Rn::mul(Rn::div(1.0, di), m_l2);
+                m_l2 = Rn::add(m_l2, Rn::mul(inv, m_l1));
+                m_l3 = Rn::mul(inv, m_l2);
                 for (int j = 0; j < a.n_snap; ++j)
                     if (a.snap_turns[j] == a.megno_idx + k && in_range)
                         a.snap[size_t(j) * n + ii] = m_l3;
@@ -164,12 +189,17 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
         }
         if (do_v) {
             double t4[4];
+            if (dev::finite_bits(v[0]) && dev::finite_bits(v[1]) && dev::finite_bits(v[2]) &&
+                dev::finite_bits(v[3])) {
+                dev::jacobian_matvec4_exact(df, v, t4);
+            } else {
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                double s = 0.0;
+                for (int r = 0; r < 4; ++r) {
+                    double s = 0.0;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) s = Rn::add(s, Rn::mul(df[r * 4 + c], v[c]));
-                t4[r] = s;
+                    for (int c = 0; c < 4; ++c) s = Rn::add(s, Rn::mul(df[r * 4 + c], v[c]));
+                    t4[r] = s;
+                }
             }
             const double nv = dev::norm_exact<4>(t4);
             if (a.n_ly) {
@@ -333,6 +363,18 @@ size_t fused_max_slots() { return 96; }
 
 cudaError_t launch_indicators(const FusedArgs &a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
+    if (!isnan(a.kick_module) || a.inverse) {
+        // whole-orbit MEGNO with kicks or backward turns
+        if (a.M == nullptr || a.V != nullptr || a.store_x != nullptr || a.n_mb != 0 ||
+            !a.df_before)
+            return cudaErrorInvalidValue;
+        const unsigned blocks = unsigned((a.n + 127) / 128);
+        if (a.mu != 0.0)
+            indicators_kernel<true, true, false, false, false, true><<<blocks, 128, 0, s>>>(a);
+        else
+            indicators_kernel<false, true, false, false, false, true><<<blocks, 128, 0, s>>>(a);
+        return cudaGetLastError();
+    }
     return a.mu != 0.0 ? launch_oct<true>(a, s) : launch_oct<false>(a, s);
 }
 

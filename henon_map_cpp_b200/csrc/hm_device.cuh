@@ -459,6 +459,42 @@ __device__ __forceinline__ void tangent_matrix_exact(double x, double y, const T
     m[15] = t.cy;
 }
 
+// Jacobian of one backward turn at the point (x, px, y, py) before it, in
+// the expression order of the reference's inverse_tangent_matrix
+// (src/henon.cu:224-249, where u and w are the coordinates after the
+// inverse rotations and pow(v, 2) is v * v).
+__device__ __forceinline__ void inverse_tangent_matrix_exact(double x, double px, double y,
+                                                             double py, const Turn &t, double mu,
+                                                             double m[16]) {
+    using R = Rn;
+    const double u = R::sub(R::mul(t.cx, x), R::mul(px, t.sx));
+    const double w = R::sub(R::mul(t.cy, y), R::mul(py, t.sy));
+    const double d2 = R::sub(R::mul(u, u), R::mul(w, w));
+    const double mu3u = R::mul(R::mul(3.0, mu), u);
+    const double gp = R::add(mu3u, 1.0);                       // 3 mu u + 1
+    const double gm = R::sub(R::mul(R::mul(-3.0, mu), u), 1.0);  // -3 mu u - 1
+    m[0] = t.cx;
+    m[1] = -t.sx;
+    m[2] = 0.0;
+    m[3] = 0.0;
+    m[4] = R::add(R::sub(R::mul(R::mul(R::mul(-3.0, t.cx), mu), d2), R::mul(R::mul(2.0, t.cx), u)),
+                  t.sx);
+    m[5] = R::add(R::add(t.cx, R::mul(R::mul(R::mul(3.0, mu), t.sx), d2)),
+                  R::mul(R::mul(2.0, t.sx), u));
+    m[6] = R::mul(R::mul(R::mul(2.0, t.cy), w), gp);
+    m[7] = R::mul(R::mul(R::mul(2.0, t.sy), w), gm);
+    m[8] = 0.0;
+    m[9] = 0.0;
+    m[10] = t.cy;
+    m[11] = -t.sy;
+    m[12] = R::mul(R::mul(R::mul(2.0, t.cx), w), gp);
+    m[13] = R::mul(R::mul(R::mul(2.0, t.sx), w), gm);
+    m[14] = R::add(R::add(R::mul(R::mul(R::mul(3.0, t.cy), mu), d2), R::mul(R::mul(2.0, t.cy), u)),
+                   t.sy);
+    m[15] = R::sub(R::sub(t.cy, R::mul(R::mul(R::mul(3.0, mu), t.sy), d2)),
+                   R::mul(R::mul(2.0, t.sy), u));
+}
+
 // out = a * b for row-major 4x4, every sum started from 0.0 and accumulated
 // in k order (get_matrices_and_multiply, src/henon.cu:279-288).
 __device__ __forceinline__ void matmul4_exact(const double a[16], const double b[16],
@@ -473,6 +509,49 @@ __device__ __forceinline__ void matmul4_exact(const double a[16], const double b
             out[i * 4 + j] = s;
         }
     }
+}
+
+// The same product for a = a turn's Jacobian (tangent_matrix_exact), whose
+// rows have one structural zero each: entry 3 of rows 0 and 1, entry 1 of
+// rows 2 and 3.  With every entry of b finite, a skipped term is 0 * b = +-0
+// and adding +-0 to a running sum that started from +0.0 never changes it
+// (the sum is never -0: x + y rounds to -0 only when both are -0), so the
+// three remaining terms, added in k order to 0.0, give the dense product's
+// bits.  The caller must fall back to matmul4_exact when b has an infinite
+// or NaN entry (0 * inf is NaN in the dense sum).
+__device__ __forceinline__ void jacobian_matmul4_exact(const double a[16], const double b[16],
+                                                       double out[16]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double b0 = b[j], b1 = b[4 + j], b2 = b[8 + j], b3 = b[12 + j];
+        out[j] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[0], b0)), Rn::mul(a[1], b1)),
+                         Rn::mul(a[2], b2));
+        out[4 + j] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[4], b0)), Rn::mul(a[5], b1)),
+                             Rn::mul(a[6], b2));
+        out[8 + j] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[8], b0)), Rn::mul(a[10], b2)),
+                             Rn::mul(a[11], b3));
+        out[12 + j] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[12], b0)), Rn::mul(a[14], b2)),
+                              Rn::mul(a[15], b3));
+    }
+}
+
+// The Jacobian applied to a vector, likewise (v finite).
+__device__ __forceinline__ void jacobian_matvec4_exact(const double a[16], const double v[4],
+                                                       double out[4]) {
+    out[0] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[0], v[0])), Rn::mul(a[1], v[1])),
+                     Rn::mul(a[2], v[2]));
+    out[1] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[4], v[0])), Rn::mul(a[5], v[1])),
+                     Rn::mul(a[6], v[2]));
+    out[2] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[8], v[0])), Rn::mul(a[10], v[2])),
+                     Rn::mul(a[11], v[3]));
+    out[3] = Rn::add(Rn::add(Rn::add(0.0, Rn::mul(a[12], v[0])), Rn::mul(a[14], v[2])),
+                     Rn::mul(a[15], v[3]));
+}
+
+// True when the double is neither infinite nor NaN (exponent field not all
+// ones), tested on the integer pipe.
+__device__ __forceinline__ bool finite_bits(double v) {
+    return (static_cast<uint32_t>(__double2hiint(v)) & 0x7ff00000u) != 0x7ff00000u;
 }
 
 // sqrt of the sum of squares from 0.0 in index order (the Frobenius norm of

@@ -275,6 +275,13 @@ struct FusedArgs {
     const uint64_t *tu_T, *tu_off;
     const double *tu_w;
     int n_tu;
+    // Whole-orbit MEGNO only (tangent matrix alone, df_before): the
+    // tracker's reproducible kicks (NaN: none; keyed by kick_seed, particle
+    // index and table index) and backward turns (table[live_step - 1 - k],
+    // steps decreasing, the Jacobian of the backward turn).
+    double kick_module;
+    unsigned long long kick_seed;
+    int inverse;
 };
 
 cudaError_t launch_indicators(const FusedArgs &a, cudaStream_t s);
@@ -362,9 +369,56 @@ struct OrbitRecordArgs {
     long long b2bits;
     int arith;
     double *ox, *opx, *oy, *opy;  // orbit [n_turns + 1][n]
+    // Optional (null when unused): each coordinate's sum over the samples,
+    // from 0.0 in sample order ([4][n]), and the first sample holding NaN
+    // (n_turns + 1 when none).
+    double *sums;
+    uint32_t *first_nan;
+    // Backward turns (table index live_step - 1 - k) and reproducible kicks
+    // (kick_module NaN: none) of particle index id0 + i.
+    int inverse;
+    double kick_module;
+    unsigned long long kick_seed;
+    size_t id0;
 };
 
 cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s);
+
+// Birkhoff tunes of the tracker's orbit in segments of turns
+// (tunes.cu): one thread per (segment, plane, particle) sums the weighted
+// phase advances of its segment for every window; a second kernel adds the
+// segments in order.  Coordinates have means[c * n + i] subtracted first
+// when means is not null.
+struct BirkhoffSegArgs {
+    const double *x, *px, *y, *py;  // orbit [S][n]
+    const double *means;            // [4][n] or null
+    const uint32_t *first_nan;      // [n]
+    size_t n, S;
+    uint32_t seg_len, n_seg;
+    const uint32_t *from, *to;  // window sample bounds (inclusive)
+    const uint64_t *w_off;
+    const double *w;
+    int n_win;
+    const uint8_t *check_nan;  // per window: NaN tune when it holds a NaN sample
+    double *partial;           // [n_win][2][n_seg][n]
+    const int *out_col;        // per window: output column pair index
+    double *out;               // [n][cols]
+    size_t cols;
+};
+cudaError_t launch_birkhoff_segments(const BirkhoffSegArgs &a, cudaStream_t s);
+
+// FFT tunes of one window of the tracker's orbit, both planes in one
+// batch: gather (mean removed, Hann window) into z[k][2n] (plane-major
+// columns, particles fastest), cuFFT, then one thread per column finds the
+// peak.
+cudaError_t launch_hann_table(double *h, uint32_t len, cudaStream_t s);
+cudaError_t launch_fft_gather2(const double *x, const double *px, const double *y,
+                               const double *py, const double *means, size_t n, uint32_t from,
+                               uint32_t len, const double *h, double2 *z, size_t S,
+                               cudaStream_t s);
+cudaError_t launch_fft_peak2(const double2 *z, uint32_t len, size_t n, uint32_t last_sample,
+                             const uint32_t *first_nan, double *out, size_t cols, int col,
+                             cudaStream_t s);
 cudaError_t launch_mean_remove(double *x, double *px, double *y, double *py, size_t n, size_t S,
                                cudaStream_t s);
 cudaError_t launch_birkhoff_tunes(const double *x, const double *px, const double *y,
@@ -387,6 +441,27 @@ hm_status particles_upload(hm_particles *p, const double *x, const double *px, c
 hm_status particles_host_mirror(const hm_particles *p);
 
 // Ghost particles and particle indices (ghosts.cu).
+// Fused ghost Lyapunov loop (ghosts.cu): n_steps steps of `every` turns,
+// each followed by the displacement log and the renormalisation of every
+// ghost, for one base particle and its ghosts per thread.  Particle j of
+// base b sits at b + n_base * j (j = 0 the base, 1..n_ghosts its ghosts).
+struct GhostLyapunovArgs {
+    double *x, *px, *y, *py;
+    uint32_t *steps;
+    size_t n_base;
+    int n_ghosts;
+    const double *table;
+    uint32_t turn0;    // table index of the first turn (the live particles' steps)
+    uint32_t every;    // turns per step
+    uint32_t n_steps;  // steps of this launch
+    double mu;
+    long long b2bits;
+    double module;
+    double *lyap;  // [n_ghosts][n_base] running sums of log(d / module)
+};
+cudaError_t launch_ghost_lyapunov(const GhostLyapunovArgs &a, int arith, cudaStream_t s);
+int ghost_lyapunov_max_ghosts();
+
 cudaError_t launch_particle_indices(uint64_t *idx, uint64_t *idx_base, size_t n, cudaStream_t s);
 cudaError_t launch_renormalize(double *x, double *px, double *y, double *py,
                                const uint64_t *idx_base, const uint8_t *ghost, size_t n,

@@ -570,8 +570,15 @@ hm_status hm_storage_get(const hm_storage *h, hm_field field, double *host_out) 
 
 // ---- fused tracking + indicators ----------------------------------------------------------
 
-hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu,
-                              double barrier, const hm_indicator_set *set) {
+}  // extern "C"
+
+namespace {
+
+// The fused construct loop; kick_module (NaN: none) and inverse only for
+// whole-orbit MEGNO (hm_tracker_megno).
+hm_status track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu,
+                           double barrier, const hm_indicator_set *set, double kick_module,
+                           bool inverse) {
     if (!t || !p || !set) return fail(HM_ERR_INVALID_ARG, "null tracker, particles or set");
     const size_t n = p->n_total;
     const hm_indicator_set &s = *set;
@@ -597,8 +604,12 @@ hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, 
     // Turn budget (src/henon.cu:3158-3167) and the table read of
     // structured_multiply after the last turn.
     const bool tangent = (s.matrix || s.vectors) && !s.jacobian_of_turn;
-    if (uint64_t(n_turns) + p->global_steps + (tangent ? 1 : 0) > t->allowed_steps)
+    if (inverse) {
+        if (n_turns > p->global_steps || n_turns > p->live_step)
+            return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    } else if (uint64_t(n_turns) + p->global_steps + (tangent ? 1 : 0) > t->allowed_steps) {
         return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    }
     if (n_turns == 0) return ok();
 
     hm::DeviceBuffer snap_turns, snap;
@@ -627,6 +638,9 @@ hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, 
     a.b2bits = 0;
     if (!std::isnan(b2)) std::memcpy(&a.b2bits, &b2, sizeof(b2));
     a.df_before = s.jacobian_of_turn ? 1 : 0;
+    a.kick_module = kick_module;
+    a.kick_seed = p->kick_seed;
+    a.inverse = inverse ? 1 : 0;
     if (s.matrix) a.M = s.matrix->m.as<double>();
     if (s.megno) {
         a.megno_l1 = s.megno->l1.as<double>();
@@ -687,8 +701,13 @@ hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, 
         a.tu_idx = s.tune ? s.tune->idx : 0;
         HM_CUDA_TRY(hm::launch_indicators(a, 0));
         HM_CUDA_TRY(cudaDeviceSynchronize());
-        p->live_step += len;
-        p->global_steps += len;
+        if (inverse) {
+            p->live_step -= len;
+            p->global_steps -= len;
+        } else {
+            p->live_step += len;
+            p->global_steps += len;
+        }
         if (s.megno) s.megno->idx += len;
         if (s.megno_birkhoff) s.megno_birkhoff->idx += len;
         if (s.lyapunov) s.lyapunov->idx += len;
@@ -703,6 +722,49 @@ hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, 
         HM_CUDA_TRY(cudaMemcpy(s.megno_samples_out, snap.ptr, s.n_megno_samples * n * sizeof(double),
                                cudaMemcpyDeviceToHost));
     return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu,
+                              double barrier, const hm_indicator_set *set) {
+    return track_indicators(t, p, n_turns, mu, barrier, set, std::nan(""), false);
+}
+
+// henon_tracker::megno (src/henon.cu:2755-2887) on the GPU, with the
+// megno_construct definition (Frobenius norm, src/henon.cu:2253-2284) of
+// the tangent map of the orbit (the Jacobian of each turn at the point
+// before it), its kick_module and inverse options included.
+hm_status hm_tracker_megno(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu,
+                           double barrier, double kick_module, int inverse,
+                           const uint64_t *turn_samples, size_t n_samples, double *host_out) {
+    if (!t || !p) return fail(HM_ERR_INVALID_ARG, "null tracker or particles");
+    if (n_samples && (!turn_samples || !host_out)) return fail(HM_ERR_INVALID_ARG, "null samples");
+    const size_t n = p->n_total;
+    hm_matrices *M = nullptr;
+    hm_megno *g = nullptr;
+    HM_TRY(hm_matrices_create(n, &M));
+    hm_status st = hm_megno_create(n, &g);
+    if (st == HM_OK) {
+        std::vector<double> snap(n_samples * n, std::nan(""));
+        hm_indicator_set s{};
+        s.matrix = M;
+        s.megno = g;
+        s.megno_sample_turns = turn_samples;
+        s.n_megno_samples = n_samples;
+        s.megno_samples_out = snap.data();
+        s.jacobian_of_turn = 1;
+        st = track_indicators(t, p, n_turns, mu, barrier, &s, kick_module, inverse != 0);
+        if (st == HM_OK)
+            for (size_t i = 0; i < n; ++i)
+                for (size_t j = 0; j < n_samples; ++j)
+                    host_out[i * n_samples + j] = snap[j * n + i];
+    }
+    hm_megno_destroy(g);
+    hm_matrices_destroy(M);
+    return st;
 }
 
 hm_status hm_storage_device_ptr(const hm_storage *h, hm_field field, const double **out) {

@@ -16,8 +16,8 @@
 // per device with cudaGetSymbolAddress (with that device current) and
 // cached.  With CUDA's lazy module loading that first lookup is also what
 // loads the device code, and so what takes the array's device memory: a
-// caller that reserves all device memory must do the set-up first
-// (hm_noalloc_prepare, or one early call).
+// caller that reserves all device memory must make one early call first
+// (n = 0 does the set-up and nothing else).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -84,10 +84,4 @@ extern "C" hm_status hm_track_device_noalloc(double *x, double *px, double *y, d
     return hm::track_driver(x, px, y, py, steps, n, tables, table_len, start_step, n_turns, mu,
                             barrier, inverse != 0, arith, scratch,
                             static_cast<cudaStream_t>(stream), &done);
-}
-
-extern "C" hm_status hm_noalloc_prepare(void) {
-    void *scratch = nullptr;
-    HM_TRY(hm::scratch_address(&scratch));
-    return hm::ok();
 }

@@ -1,6 +1,7 @@
 // Ghost particles and host-side tangent matrices of the particle API
 // (particles_4d[_gpu]::add_ghost / renormalize / get_displacement_*,
 // henon_tracker_gpu::get_tangent_matrix).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -155,6 +156,71 @@ hm_status hm_particles_displacement_module(const hm_particles *p, double *host_o
     for (size_t b = 0; b < nb; ++b)
         for (size_t k = 0; k < ng; ++k) host_out[b * ng + k] = g[k * nb + b];
     return ok();
+}
+
+// The ghost Lyapunov loop of tests/test_new_standard.ipynb:477-479 (track
+// `every` turns, accumulate log(displacement / module), renormalize) in
+// fused launches (ghosts.cu).  host_out: double[n_particles][n_ghosts],
+// the sums over this call's steps.
+hm_status hm_track_ghost_lyapunov(hm_tracker *t, hm_particles *p, uint32_t n_steps,
+                                  uint32_t every, double mu, double barrier, double module,
+                                  double *host_out) {
+    if (!t || !p) return fail(HM_ERR_INVALID_ARG, "null tracker or particles");
+    const size_t nb = p->n_particles, ng = p->n_ghosts;
+    if (ng == 0) return fail(HM_ERR_INVALID_ARG, "the particles have no ghosts (add_ghost first)");
+    if (ng > size_t(hm::ghost_lyapunov_max_ghosts()))
+        return fail(HM_ERR_NOT_SUPPORTED, "at most " +
+                                              std::to_string(hm::ghost_lyapunov_max_ghosts()) +
+                                              " ghosts per particle in the fused ghost loop");
+    if (every == 0) return fail(HM_ERR_INVALID_ARG, "every must be positive");
+    if (p->n_total != nb * (1 + ng)) return fail(HM_ERR_INVALID_ARG, "inconsistent ghost layout");
+    const uint64_t turns = uint64_t(n_steps) * every;
+    if (turns + p->global_steps > t->allowed_steps || turns > 0xffffffffull)
+        return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    if (nb == 0 || n_steps == 0) return ok();
+    if (!host_out) return fail(HM_ERR_INVALID_ARG, "null output");
+    DeviceBuffer lyap;
+    HM_TRY(lyap.alloc(nb * ng * sizeof(double)));
+    HM_CUDA_TRY(cudaMemsetAsync(lyap.ptr, 0, nb * ng * sizeof(double), 0));
+    hm::GhostLyapunovArgs a{};
+    a.x = p->x.as<double>();
+    a.px = p->px.as<double>();
+    a.y = p->y.as<double>();
+    a.py = p->py.as<double>();
+    a.steps = p->steps.as<uint32_t>();
+    a.n_base = nb;
+    a.n_ghosts = int(ng);
+    a.table = t->table.as<const double>();
+    a.every = every;
+    a.mu = mu;
+    const double b2 = barrier * barrier;
+    a.b2bits = 0;
+    if (!std::isnan(b2)) std::memcpy(&a.b2bits, &b2, sizeof(b2));
+    a.module = module;
+    a.lyap = lyap.as<double>();
+    // Launches of whole steps, about 4096 turns each (cancellation is
+    // checked between them).
+    const uint32_t per_launch = std::max<uint32_t>(1u, 4096u / every);
+    uint32_t done = 0;
+    hm_status status = HM_OK;
+    while (done < n_steps) {
+        a.turn0 = p->live_step;
+        a.n_steps = std::min(per_launch, n_steps - done);
+        HM_CUDA_TRY(hm::launch_ghost_lyapunov(a, t->arith, 0));
+        HM_CUDA_TRY(cudaStreamSynchronize(0));
+        done += a.n_steps;
+        p->global_steps += a.n_steps * every;
+        p->live_step += a.n_steps * every;
+        if (done < n_steps && hm::cancel_requested()) {
+            status = fail(HM_ERR_CANCELLED, "ghost loop cancelled");
+            break;
+        }
+    }
+    std::vector<double> g(nb * ng);  // [ghost][base]
+    HM_CUDA_TRY(cudaMemcpy(g.data(), lyap.ptr, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t b = 0; b < nb; ++b)
+        for (size_t k = 0; k < ng; ++k) host_out[b * ng + k] = g[k * nb + b];
+    return status == HM_OK ? ok() : status;
 }
 
 // get_displacement_direction (src/henon.cu:1345-1442): host

@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -20,6 +22,12 @@ using hm::ok;
 struct hm_storage;  // defined in indicators.cpp
 extern "C" hm_status hm_storage_device_ptr(const hm_storage *h, hm_field field, const double **out);
 extern "C" hm_status hm_storage_size(const hm_storage *h, size_t *n, size_t *batch, size_t *stored);
+
+#define HM_CUFFT_TRY_STREAM(plan)                                           \
+    do {                                                                    \
+        const cufftResult _r = cufftSetStream((plan), 0);                   \
+        if (_r != CUFFT_SUCCESS) return cufft_fail(_r, "set stream");       \
+    } while (0)
 
 namespace {
 
@@ -163,34 +171,164 @@ hm_status hm_orbit_tunes_host(const double *x, const double *px, const double *y
                           d[3].as<double>(), n, n_samples, from, to, n_windows, method, host_out);
 }
 
+}  // extern "C"
+
+namespace {
+
+// cuFFT plans of the tracker's tune path, kept across calls: one per
+// (device, length, batch), with the particle-fastest layout of
+// fft_gather2 (element k of column c at k * batch + c).  Creating a plan
+// costs more than running it at these sizes.
+struct PlanCache {
+    std::mutex mutex;
+    std::map<std::tuple<int, uint32_t, size_t>, cufftHandle> plans;
+    ~PlanCache() {
+        for (auto &kv : plans) cufftDestroy(kv.second);
+    }
+};
+
+PlanCache &plan_cache() {
+    static PlanCache c;
+    return c;
+}
+
+hm_status strided_plan(uint32_t len, size_t batch, cufftHandle *out) {
+    int dev = 0;
+    HM_CUDA_TRY(cudaGetDevice(&dev));
+    PlanCache &c = plan_cache();
+    std::lock_guard<std::mutex> lock(c.mutex);
+    const auto key = std::make_tuple(dev, len, batch);
+    auto it = c.plans.find(key);
+    if (it != c.plans.end()) {
+        *out = it->second;
+        return ok();
+    }
+    if (c.plans.size() >= 16) {  // bounded: drop the whole cache
+        for (auto &kv : c.plans) cufftDestroy(kv.second);
+        c.plans.clear();
+    }
+    cufftHandle plan = 0;
+    int nl = int(len);
+    const int stride = int(batch);
+    const cufftResult r = cufftPlanMany(&plan, 1, &nl, &nl, stride, 1, &nl, stride, 1, CUFFT_Z2Z,
+                                        int(batch));
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "strided plan");
+    c.plans[key] = plan;
+    *out = plan;
+    return ok();
+}
+
+// One tune window of the tracker path: inclusive sample bounds, the NaN
+// rule, and the output column pair it fills.
+struct Window {
+    uint32_t from, to;
+    bool check_nan;
+    std::vector<int> cols;
+};
+
+// Equal windows are computed once and written to every column pair they
+// serve (the engine appends [0, n_turns], which equals the full orbit).
+void add_window(std::vector<Window> &ws, uint32_t from, uint32_t to, bool check_nan, int col) {
+    for (Window &w : ws)
+        if (w.from == from && w.to == to && w.check_nan == check_nan) {
+            w.cols.push_back(col);
+            return;
+        }
+    ws.push_back(Window{from, to, check_nan, {col}});
+}
+
+}  // namespace
+
+extern "C" {
+
 // Tracks n_turns turns recording the orbit (sample 0 = the current state),
 // optionally removes each orbit's mean, and returns Birkhoff tunes (and FFT
 // tunes when fft_out) of the windows plus the full orbit:
 // henon_tracker::birkhoff_tunes (remove_mean = 0) and ::all_tunes
-// (remove_mean = 1), src/henon.cu:2890-3078.  Outputs host
-// double[n_total][2 (n_windows + 1)].
+// (remove_mean = 1), src/henon.cu:2890-3078, with their kick_module and
+// inverse options.  Outputs host double[n_total][2 (n_windows + 1)].
 hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turns, double mu,
-                                 double barrier, const uint32_t *from, const uint32_t *to,
-                                 size_t n_windows, int remove_mean, double *birkhoff_out,
-                                 double *fft_out) {
+                                 double barrier, double kick_module, int inverse,
+                                 const uint32_t *from, const uint32_t *to, size_t n_windows,
+                                 int remove_mean, double *birkhoff_out, double *fft_out) {
     if (!t || !p) return fail(HM_ERR_INVALID_ARG, "null tracker or particles");
-    if (uint64_t(n_turns) + p->global_steps > t->allowed_steps)
+    if (inverse) {
+        if (n_turns > p->global_steps || n_turns > p->live_step)
+            return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    } else if (uint64_t(n_turns) + p->global_steps > t->allowed_steps) {
         return fail(HM_ERR_BUDGET, "The number of turns is too large.");
+    }
     if (n_turns == 0) return fail(HM_ERR_INVALID_ARG, "need at least one turn");
     const size_t S = size_t(n_turns) + 1;
     HM_TRY(check_windows(S, from, to, n_windows));
     const size_t n = p->n_total;
     if (n && !birkhoff_out) return fail(HM_ERR_INVALID_ARG, "null output");
-    const std::vector<uint32_t> f(from, from + n_windows), tt(to, to + n_windows);
     const size_t cols = 2 * (n_windows + 1);
-    // Orbit slice: at most half the free device memory.
+    // Birkhoff windows: the caller's (NaN when they hold a NaN sample) and
+    // the full orbit [0, S-1] (no check: NaN propagates through the sums).
+    // FFT windows: the caller's, and the full orbit's samples 1..S-1 (NaN
+    // when any sample is).
+    std::vector<Window> bw, fw;
+    for (size_t j = 0; j < n_windows; ++j) {
+        add_window(bw, from[j], to[j], true, int(j));
+        add_window(fw, from[j], to[j], true, int(j));
+    }
+    add_window(bw, 0, uint32_t(S - 1), false, int(n_windows));
+    add_window(fw, 1, uint32_t(S - 1), true, int(n_windows));
+    // Expanded per column pair for the Birkhoff finish kernel.
+    std::vector<uint32_t> bf, bt;
+    std::vector<uint8_t> bchk;
+    std::vector<int> bcol;
+    std::vector<uint64_t> boff;
+    std::vector<double> bwts;
+    for (const Window &w : bw) {
+        auto ww = hm::birkhoff_weights(w.to - w.from);
+        for (int c : w.cols) {
+            bf.push_back(w.from);
+            bt.push_back(w.to);
+            bchk.push_back(w.check_nan ? 1 : 0);
+            bcol.push_back(c);
+            boff.push_back(bwts.size());
+            bwts.insert(bwts.end(), ww.begin(), ww.end());
+        }
+    }
+    DeviceBuffer d_bf, d_bt, d_bchk, d_bcol, d_boff, d_bw;
+    HM_TRY(hm::upload(d_bf, bf));
+    HM_TRY(hm::upload(d_bt, bt));
+    HM_TRY(hm::upload(d_bchk, bchk));
+    HM_TRY(hm::upload(d_bcol, bcol));
+    HM_TRY(hm::upload(d_boff, boff));
+    HM_TRY(hm::upload(d_bw, bwts));
+    // Hann tables of the FFT windows.
+    uint32_t max_len = 0;
+    std::vector<DeviceBuffer> hann(fw.size());
+    if (fft_out) {
+        for (size_t j = 0; j < fw.size(); ++j) {
+            const uint32_t L = fw[j].to - fw[j].from + 1;
+            max_len = std::max(max_len, L);
+            HM_TRY(hann[j].alloc(size_t(L) * sizeof(double)));
+            HM_CUDA_TRY(hm::launch_hann_table(hann[j].as<double>(), L, 0));
+        }
+    }
+    // Particle slice: the orbit (32 B per sample) plus the largest FFT
+    // window of both planes (32 B per sample) in at most two thirds of the
+    // free device memory.
     size_t free_b = 0;
     HM_TRY(hm::device_free_bytes(&free_b));
-    const size_t per_particle = S * 4 * sizeof(double);
-    const size_t slice = std::max<size_t>(1, std::min<size_t>(n, (free_b / 2) / per_particle));
-    DeviceBuffer orbit, out;
-    HM_TRY(orbit.alloc(std::min(n, slice) * per_particle));
-    HM_TRY(out.alloc(cols * std::min(n, slice) * sizeof(double)));
+    const size_t per_particle = S * 4 * sizeof(double) + size_t(max_len) * 2 * sizeof(double2);
+    const size_t slice = std::max<size_t>(1, std::min<size_t>(n, (free_b / 3 * 2) / per_particle));
+    const size_t m0 = std::min(n, slice);
+    // Segments of the Birkhoff sums: enough threads to fill the device.
+    const uint32_t seg_len = std::max<uint32_t>(64u, uint32_t(std::min<size_t>(
+                                                         S, (S * m0 * 2 + 262143) / 262144)));
+    const uint32_t n_seg = uint32_t((S - 1 + seg_len - 1) / seg_len);
+    DeviceBuffer orbit, out, sums, first_nan, partial, z;
+    HM_TRY(orbit.alloc(m0 * S * 4 * sizeof(double)));
+    HM_TRY(out.alloc(cols * m0 * sizeof(double)));
+    if (remove_mean) HM_TRY(sums.alloc(4 * m0 * sizeof(double)));
+    HM_TRY(first_nan.alloc(m0 * sizeof(uint32_t)));
+    HM_TRY(partial.alloc(bf.size() * 2 * size_t(std::max<uint32_t>(n_seg, 1)) * m0 * sizeof(double)));
+    if (fft_out) HM_TRY(z.alloc(size_t(max_len) * 2 * m0 * sizeof(double2)));
     const double b2 = barrier * barrier;
     long long b2bits = 0;
     if (!std::isnan(b2)) std::memcpy(&b2bits, &b2, sizeof(b2));
@@ -214,19 +352,66 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
         a.opx = o + S * m;
         a.oy = o + 2 * S * m;
         a.opy = o + 3 * S * m;
+        a.sums = remove_mean ? sums.as<double>() : nullptr;
+        a.first_nan = first_nan.as<uint32_t>();
+        a.inverse = inverse != 0;
+        a.kick_module = kick_module;
+        a.kick_seed = p->kick_seed;
+        a.id0 = first;
         HM_CUDA_TRY(hm::launch_orbit_record(a, 0));
-        if (remove_mean) HM_CUDA_TRY(hm::launch_mean_remove(a.ox, a.opx, a.oy, a.opy, m, S, 0));
-        HM_TRY(birkhoff_device(a.ox, a.opx, a.oy, a.opy, m, S, f, tt, out.as<double>()));
+        const double *means = remove_mean ? sums.as<double>() : nullptr;
+
+        hm::BirkhoffSegArgs g{};
+        g.x = a.ox;
+        g.px = a.opx;
+        g.y = a.oy;
+        g.py = a.opy;
+        g.means = means;
+        g.first_nan = a.first_nan;
+        g.n = m;
+        g.S = S;
+        g.seg_len = seg_len;
+        g.n_seg = n_seg;
+        g.from = d_bf.as<uint32_t>();
+        g.to = d_bt.as<uint32_t>();
+        g.w_off = d_boff.as<uint64_t>();
+        g.w = d_bw.as<double>();
+        g.n_win = int(bf.size());
+        g.check_nan = d_bchk.as<uint8_t>();
+        g.partial = partial.as<double>();
+        g.out_col = d_bcol.as<int>();
+        g.out = out.as<double>();
+        g.cols = cols;
+        HM_CUDA_TRY(hm::launch_birkhoff_segments(g, 0));
         HM_CUDA_TRY(cudaMemcpy(birkhoff_out + first * cols, out.ptr, m * cols * sizeof(double),
                                cudaMemcpyDeviceToHost));
         if (fft_out) {
-            HM_TRY(fft_device(a.ox, a.opx, a.oy, a.opy, m, S, f, tt, out.as<double>()));
+            for (size_t j = 0; j < fw.size(); ++j) {
+                const uint32_t L = fw[j].to - fw[j].from + 1;
+                auto *zz = z.as<double2>();
+                HM_CUDA_TRY(hm::launch_fft_gather2(a.ox, a.opx, a.oy, a.opy, means, m, fw[j].from,
+                                                   L, hann[j].as<double>(), zz, S, 0));
+                cufftHandle plan = 0;
+                HM_TRY(strided_plan(L, 2 * m, &plan));
+                HM_CUFFT_TRY_STREAM(plan);
+                auto *zc = reinterpret_cast<cufftDoubleComplex *>(zz);
+                const cufftResult r = cufftExecZ2Z(plan, zc, zc, CUFFT_FORWARD);
+                if (r != CUFFT_SUCCESS) return cufft_fail(r, "exec");
+                for (int c : fw[j].cols)
+                    HM_CUDA_TRY(hm::launch_fft_peak2(zz, L, m, fw[j].to, a.first_nan,
+                                                     out.as<double>(), cols, c, 0));
+            }
             HM_CUDA_TRY(cudaMemcpy(fft_out + first * cols, out.ptr, m * cols * sizeof(double),
                                    cudaMemcpyDeviceToHost));
         }
     }
-    p->global_steps += n_turns;
-    p->live_step += n_turns;
+    if (inverse) {
+        p->global_steps -= n_turns;
+        p->live_step -= n_turns;
+    } else {
+        p->global_steps += n_turns;
+        p->live_step += n_turns;
+    }
     return ok();
 }
 

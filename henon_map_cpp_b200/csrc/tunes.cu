@@ -15,6 +15,13 @@
 // * hann_gather_kernel + cuFFT + fft_peak_kernel: Hann-windowed spectrum of
 //   x + i px and the interpolated peak (compute_fft, interpolation, A,
 //   fft_tune_vec, src/dynamic_indicator.cpp:32-61, 134-196, 255-330).
+// Those serve orbits the caller stored (storage tunes).  The tracker's own
+// tune path records the orbit with each coordinate's running sum and the
+// first NaN sample, and then never rewrites it: the mean is subtracted as
+// samples are read, Birkhoff sums run in segments of turns over many
+// threads (birkhoff_seg_kernel / birkhoff_finish_kernel), and the FFT
+// gather writes both planes of a window as one batch with particles
+// fastest (fft_gather2_kernel, fft_peak2_kernel).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -27,7 +34,14 @@ namespace {
 
 using dev::Rn;
 
-template <int ARITH, bool OCT>
+// Tracks n_turns turns and writes every state (sample 0 = the start).  The
+// turn is the tracker's: forward with table[live_step + k], or backward with
+// table[live_step - 1 - k] (REV), with the tracker's reproducible kicks
+// (KICK: added before the forward turn, subtracted after the backward
+// one).  Optionally each coordinate's sum over the samples (from 0.0, in
+// sample order: the reference's std::accumulate for all_tunes' mean,
+// src/henon.cu:3040-3051) and the first NaN sample.
+template <int ARITH, bool OCT, bool REV, bool KICK>
 __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
@@ -35,17 +49,32 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     double x = a.x[i], px = a.px[i], y = a.y[i], py = a.py[i];
     uint32_t steps = a.steps[i];
     bool alive = !dev::is_lost(x, px, y, py);
+    uint32_t first_nan = alive ? a.n_turns + 1u : 0u;
     a.ox[i] = x;
     a.opx[i] = px;
     a.oy[i] = y;
     a.opy[i] = py;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    const bool sums = a.sums != nullptr;
+    if (sums) {
+        s0 = Rn::add(s0, x);
+        s1 = Rn::add(s1, px);
+        s2 = Rn::add(s2, y);
+        s3 = Rn::add(s3, py);
+    }
     dev::Particle p = dev::make_particle(x, px, y, py);
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
+    const unsigned long long id = a.id0 + i;
     for (uint32_t k = 0; k < a.n_turns; ++k) {
         if (alive) {
-            dev::turn<ARITH, OCT, false>(p, dev::load_turn(a.table, a.live_step + k), a.mu);
+            const uint32_t idx = REV ? a.live_step - 1u - k : a.live_step + k;
+            if (KICK && !REV)
+                dev::apply_kick<false>(p, dev::kick_direction(a.kick_seed, id, idx), a.kick_module);
+            dev::turn<ARITH, OCT, REV>(p, dev::load_turn(a.table, idx), a.mu);
+            if (KICK && REV)
+                dev::apply_kick<true>(p, dev::kick_direction(a.kick_seed, id, idx), a.kick_module);
             if (dev::inside_after_turn<ARITH>(p, bar)) {
-                steps += 1u;
+                steps = REV ? steps - 1u : steps + 1u;
                 x = p.x;
                 px = p.px;
                 y = p.y;
@@ -53,6 +82,7 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
             } else {
                 x = px = y = py = dev::quiet_nan();
                 alive = false;
+                first_nan = k + 1u;
             }
         }
         const size_t o = size_t(k + 1) * n + i;
@@ -60,12 +90,196 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
         a.opx[o] = px;
         a.oy[o] = y;
         a.opy[o] = py;
+        if (sums) {
+            s0 = Rn::add(s0, x);
+            s1 = Rn::add(s1, px);
+            s2 = Rn::add(s2, y);
+            s3 = Rn::add(s3, py);
+        }
     }
     a.x[i] = x;
     a.px[i] = px;
     a.y[i] = y;
     a.py[i] = py;
     a.steps[i] = steps;
+    if (sums) {
+        a.sums[i] = s0;
+        a.sums[n + i] = s1;
+        a.sums[2 * n + i] = s2;
+        a.sums[3 * n + i] = s3;
+    }
+    if (a.first_nan) a.first_nan[i] = first_nan;
+}
+
+__device__ double interp_a(double a, double b, double c);
+
+// mean = sum / samples, as the reference divides std::accumulate's result.
+__device__ __forceinline__ double mean_of(const double *means, size_t n, size_t i, int c,
+                                          size_t S) {
+    return means ? Rn::div(means[size_t(c) * n + i], double(S)) : 0.0;
+}
+
+// v - mean, separately rounded (the reference subtracts the mean from every
+// stored sample); without a mean the sample itself.
+__device__ __forceinline__ double centred(double v, const double *means, double m) {
+    return means ? Rn::sub(v, m) : v;
+}
+
+// Birkhoff phase-advance sums of one segment of turns [s0, s1) for one plane
+// of one particle, every window at once: the transition s -> s+1 adds
+// w_j[s - from_j] dtheta_s to window j when from_j <= s < to_j, dtheta
+// wrapped by +2 pi when negative (birkhoff_tune,
+// src/dynamic_indicator.cpp:81-131).  Windows in groups of kWinGroup
+// (blockIdx.y) so that the sums stay in registers.
+constexpr int kWinGroup = 8;
+
+__global__ void birkhoff_seg_kernel(const BirkhoffSegArgs a) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t n = a.n;
+    const size_t sp = t / n;  // segment * 2 + plane
+    if (sp >= 2u * size_t(a.n_seg)) return;
+    const size_t i = t - sp * n;
+    const uint32_t seg = uint32_t(sp >> 1);
+    const int plane = int(sp & 1u);
+    const int w0 = int(blockIdx.y) * kWinGroup;
+    const int nw = min(kWinGroup, a.n_win - w0);
+    const double *q = plane ? a.y : a.x, *p = plane ? a.py : a.px;
+    const double mq = mean_of(a.means, n, i, 2 * plane, a.S);
+    const double mp = mean_of(a.means, n, i, 2 * plane + 1, a.S);
+    const uint32_t s0 = seg * a.seg_len;
+    const uint32_t s1 = min(uint32_t(a.S - 1), s0 + a.seg_len);
+    uint32_t lo[kWinGroup], hi[kWinGroup];
+    long long wb[kWinGroup];  // weight of transition s: w[wb + s]
+    double acc[kWinGroup];
+#pragma unroll
+    for (int j = 0; j < kWinGroup; ++j) {
+        acc[j] = 0.0;
+        lo[j] = 1u;  // empty window
+        hi[j] = 0u;
+        wb[j] = 0;
+        if (j < nw) {
+            lo[j] = a.from[w0 + j];
+            hi[j] = a.to[w0 + j];
+            wb[j] = (long long)a.w_off[w0 + j] - (long long)lo[j];
+        }
+    }
+    double prev = atan2(centred(p[size_t(s0) * n + i], a.means, mp),
+                        centred(q[size_t(s0) * n + i], a.means, mq));
+    for (uint32_t s = s0; s < s1; ++s) {
+        const size_t o = size_t(s + 1) * n + i;
+        const double th = atan2(centred(p[o], a.means, mp), centred(q[o], a.means, mq));
+        double d = Rn::sub(th, prev);
+        if (d < 0.0) d = Rn::add(d, 2.0 * M_PI);
+        prev = th;
+#pragma unroll
+        for (int j = 0; j < kWinGroup; ++j)
+            if (s >= lo[j] && s < hi[j]) acc[j] = Rn::add(acc[j], Rn::mul(a.w[wb[j] + s], d));
+    }
+#pragma unroll
+    for (int j = 0; j < kWinGroup; ++j)
+        if (j < nw)
+            a.partial[((size_t(w0 + j) * 2 + plane) * a.n_seg + seg) * n + i] = acc[j];
+}
+
+// 1 - (sum of the segments' sums, in segment order) / (2 pi); NaN for a
+// window marked check_nan that holds a NaN sample (birkhoff_tune_vec checks
+// the caller's windows, not the appended full orbit).
+__global__ void birkhoff_finish_kernel(const BirkhoffSegArgs a) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t n = a.n;
+    const size_t wp = t / n;  // window * 2 + plane
+    if (wp >= 2u * size_t(a.n_win)) return;
+    const size_t i = t - wp * n;
+    const int j = int(wp >> 1), plane = int(wp & 1u);
+    const double *part = a.partial + (size_t(j) * 2 + plane) * a.n_seg * n + i;
+    double sum = 0.0;
+    for (uint32_t g = 0; g < a.n_seg; ++g) sum = Rn::add(sum, part[size_t(g) * n]);
+    double tune = Rn::sub(1.0, Rn::div(sum, Rn::mul(2.0, M_PI)));
+    if (a.check_nan[j] && a.first_nan[i] <= a.to[j]) tune = dev::quiet_nan();
+    a.out[i * a.cols + 2 * size_t(a.out_col[j]) + plane] = tune;
+}
+
+// Hann window 2 sin^2(pi k / len) (compute_fft, src/dynamic_indicator.cpp:
+// 32-61), the same expression as hann_gather_kernel's.
+__global__ void hann_table_kernel(double *h, uint32_t len) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= len) return;
+    const double s = sin(M_PI * double(k) / double(len));
+    h[k] = 2 * pow(s, 2);
+}
+
+// z[k][plane n + i] = ((q - mean) + i (p - mean)) h_k over the window's
+// samples from .. from + len - 1; consecutive threads take consecutive
+// particles (coalesced orbit reads and spectrum writes).
+__global__ void fft_gather2_kernel(const double *x, const double *px, const double *y,
+                                   const double *py, const double *means, size_t n,
+                                   uint32_t from, uint32_t len, const double *h, double2 *z,
+                                   size_t S) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t cols = 2 * n;
+    if (t >= size_t(len) * cols) return;
+    const size_t k = t / cols, c = t - k * cols;
+    const int plane = c >= n ? 1 : 0;
+    const size_t i = c - size_t(plane) * n;
+    const double *q = plane ? y : x, *p = plane ? py : px;
+    const size_t o = size_t(from + k) * n + i;
+    const double re = centred(q[o], means, mean_of(means, n, i, 2 * plane, S));
+    const double im = centred(p[o], means, mean_of(means, n, i, 2 * plane + 1, S));
+    const double hk = h[k];
+    z[t] = make_double2(re * hk, im * hk);
+}
+
+// One thread per column (plane, particle): first maximum of |z_k| over k,
+// then the interpolation of src/dynamic_indicator.cpp:139-176 -> |1 - v|;
+// NaN when the window's samples from .. last_sample hold a NaN.
+__global__ void fft_peak2_kernel(const double2 *z, uint32_t len, size_t n, uint32_t last_sample,
+                                 const uint32_t *first_nan, double *out, size_t out_cols,
+                                 int col) {
+    const size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t cols = 2 * n;
+    if (c >= cols) return;
+    const int plane = c >= n ? 1 : 0;
+    const size_t i = c - size_t(plane) * n;
+    auto mag = [&](uint32_t k) {
+        const double2 v = z[size_t(k) * cols + c];
+        return sqrt(v.x * v.x + v.y * v.y);
+    };
+    double value;
+    if (first_nan[i] <= last_sample) {
+        value = dev::quiet_nan();
+    } else {
+        double best = -1.0;
+        uint32_t index = 0;
+        for (uint32_t k = 0; k < len; ++k) {
+            const double m = mag(k);
+            if (m > best) {
+                best = m;
+                index = k;
+            }
+        }
+        const double N = double(len);
+        if (index == 0) {
+            value = 1.0;
+        } else if (index == len - 1) {
+            value = 0.0;
+        } else {
+            uint32_t i1, i2;
+            if (mag(index - 1) > mag(index + 1)) {
+                i1 = index - 1;
+                i2 = index;
+                index = index - 1;
+            } else {
+                i1 = index;
+                i2 = index + 1;
+            }
+            const double v = (double(index) / N) +
+                             (1.0 / (2.0 * M_PI)) *
+                                 asin(interp_a(mag(i1), mag(i2), cos(2.0 * M_PI / N)) *
+                                      sin(2.0 * M_PI / N));
+            value = fabs(1.0 - v);
+        }
+    }
+    out[i * out_cols + 2 * size_t(col) + plane] = value;
 }
 
 // v -= mean(v) per particle and coordinate, one thread per (coordinate,
@@ -226,19 +440,72 @@ __global__ void fft_peak_kernel(const double2 *buf, uint32_t len, size_t count,
     out[(first + warp) * out_stride] = value;
 }
 
+template <int ARITH, bool OCT>
+void launch_record_ok(const OrbitRecordArgs &a, unsigned blocks, int threads, cudaStream_t s) {
+    const bool kick = !isnan(a.kick_module);
+    if (a.inverse) {
+        if (kick) orbit_record_kernel<ARITH, OCT, true, true><<<blocks, threads, 0, s>>>(a);
+        else orbit_record_kernel<ARITH, OCT, true, false><<<blocks, threads, 0, s>>>(a);
+    } else {
+        if (kick) orbit_record_kernel<ARITH, OCT, false, true><<<blocks, threads, 0, s>>>(a);
+        else orbit_record_kernel<ARITH, OCT, false, false><<<blocks, threads, 0, s>>>(a);
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    const unsigned blocks = unsigned((a.n + 127) / 128);
+    // Small blocks: the orbit of few particles is a long serial chain, so
+    // spread the threads over as many SMs as possible.
+    const int threads = a.n < 148u * 128u ? 32 : 128;
+    const unsigned blocks = unsigned((a.n + threads - 1) / threads);
     const bool oct = a.mu != 0.0;
     if (a.arith == HM_ARITH_FAST) {
-        if (oct) orbit_record_kernel<HM_ARITH_FAST, true><<<blocks, 128, 0, s>>>(a);
-        else orbit_record_kernel<HM_ARITH_FAST, false><<<blocks, 128, 0, s>>>(a);
+        if (oct) launch_record_ok<HM_ARITH_FAST, true>(a, blocks, threads, s);
+        else launch_record_ok<HM_ARITH_FAST, false>(a, blocks, threads, s);
     } else {
-        if (oct) orbit_record_kernel<HM_ARITH_EXACT, true><<<blocks, 128, 0, s>>>(a);
-        else orbit_record_kernel<HM_ARITH_EXACT, false><<<blocks, 128, 0, s>>>(a);
+        if (oct) launch_record_ok<HM_ARITH_EXACT, true>(a, blocks, threads, s);
+        else launch_record_ok<HM_ARITH_EXACT, false>(a, blocks, threads, s);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_birkhoff_segments(const BirkhoffSegArgs &a, cudaStream_t s) {
+    if (a.n == 0 || a.n_win == 0) return cudaSuccess;
+    const size_t threads = 2u * size_t(a.n_seg) * a.n;
+    const dim3 grid(unsigned((threads + 127) / 128), unsigned((a.n_win + kWinGroup - 1) / kWinGroup));
+    birkhoff_seg_kernel<<<grid, 128, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t t2 = 2u * size_t(a.n_win) * a.n;
+    birkhoff_finish_kernel<<<unsigned((t2 + 127) / 128), 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hann_table(double *h, uint32_t len, cudaStream_t s) {
+    if (len == 0) return cudaSuccess;
+    hann_table_kernel<<<(len + 255) / 256, 256, 0, s>>>(h, len);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_gather2(const double *x, const double *px, const double *y,
+                               const double *py, const double *means, size_t n, uint32_t from,
+                               uint32_t len, const double *h, double2 *z, size_t S,
+                               cudaStream_t s) {
+    const size_t total = size_t(len) * 2 * n;
+    if (total == 0) return cudaSuccess;
+    fft_gather2_kernel<<<unsigned((total + 255) / 256), 256, 0, s>>>(x, px, y, py, means, n,
+                                                                      from, len, h, z, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_peak2(const double2 *z, uint32_t len, size_t n, uint32_t last_sample,
+                             const uint32_t *first_nan, double *out, size_t cols, int col,
+                             cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    fft_peak2_kernel<<<unsigned((2 * n + 127) / 128), 128, 0, s>>>(z, len, n, last_sample,
+                                                                    first_nan, out, cols, col);
     return cudaGetLastError();
 }
 

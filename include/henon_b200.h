@@ -197,6 +197,24 @@ hm_status hm_particles_displacement_module(const hm_particles *p,
 /* get_displacement_direction (:1345-1442): double[4][n_particles][n_ghosts]. */
 hm_status hm_particles_displacement_direction(const hm_particles *p,
                                               double *host_out);
+/* The displacement (ghost) Lyapunov loop of the reference's notebooks
+ * (tests/test_new_standard.ipynb:477-479), which a Python caller runs as
+ *     for step in range(n_steps):
+ *         tracker.track(p, every, mu, barrier)
+ *         lyap += log(p.get_displacement_module() / module)
+ *         p.renormalize(module)
+ * over add_ghost / renormalize / get_displacement_module (src/henon.cu:
+ * 737-818, 1257-1343), in fused launches: each thread carries a base
+ * particle and its ghosts in registers.  Coordinates, steps and
+ * global_steps end as after that loop, bit for bit; host_out
+ * (double[n_particles][n_ghosts]) receives the sums of log(d / module)
+ * over this call's steps (CUDA's log: each term within an ulp of the host
+ * loop's).  1 to 4 ghosts per particle (HM_ERR_NOT_SUPPORTED beyond).  No
+ * kicks.  Synchronous; cancellable between launches. */
+hm_status hm_track_ghost_lyapunov(hm_tracker *t, hm_particles *p,
+                                  uint32_t n_steps, uint32_t every, double mu,
+                                  double barrier, double module,
+                                  double *host_out);
 /* henon_tracker_gpu::get_tangent_matrix (src/henon.cu:3187-3219), computed
  * on the host like the reference: double[n_total][16]. */
 hm_status hm_tracker_tangent_matrices(const hm_tracker *t,
@@ -385,6 +403,18 @@ typedef struct hm_indicator_set {
 hm_status hm_track_indicators(hm_tracker *t, hm_particles *p, uint32_t n_turns,
                               double mu, double barrier,
                               const hm_indicator_set *set);
+/* henon_tracker::megno (src/henon.cu:2755-2887) on the GPU: MEGNO of the
+ * tangent map of the orbit (the Jacobian of each turn at the point before
+ * it, accumulated as megno_construct does, src/henon.cu:2253-2284) at the
+ * turn counts turn_samples, host_out double[n_total][n_samples].  As in the
+ * reference the call tracks the particles n_turns turns, with kick_module
+ * (NaN: none; hm_track's reproducible kicks) and inverse (backward turns,
+ * each with the Jacobian of the backward turn, inverse_tangent_matrix
+ * src/henon.cu:224-249; global_steps decreases). */
+hm_status hm_tracker_megno(hm_tracker *t, hm_particles *p, uint32_t n_turns,
+                           double mu, double barrier, double kick_module,
+                           int inverse, const uint64_t *turn_samples,
+                           size_t n_samples, double *host_out);
 
 /* ---- batched heterogeneous tracking ---------------------------------------
  * Replaces the reference's one-process-per-parameter-set sweeps
@@ -463,10 +493,14 @@ hm_status hm_orbit_tunes_host(const double *x, const double *px, const double *y
  * then Birkhoff tunes (and FFT tunes when fft_out is not NULL) of the
  * windows plus the full orbit, with each orbit's mean removed first when
  * remove_mean: henon_tracker::birkhoff_tunes (remove_mean 0) and
- * ::all_tunes (remove_mean 1), src/henon.cu:2890-3078.  Outputs host
- * double[n_total][2 (n_windows + 1)]. */
+ * ::all_tunes (remove_mean 1), src/henon.cu:2890-3078.  kick_module (NaN:
+ * none) and inverse are hm_track's: reproducible kicks keyed by the
+ * particles' kick_seed, backward turns with global_steps decreasing.
+ * Outputs host double[n_total][2 (n_windows + 1)].  Birkhoff sums are
+ * added in segments of turns (within 1e-13 of the sequential sum). */
 hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turns,
-                                 double mu, double barrier, const uint32_t *from,
+                                 double mu, double barrier, double kick_module,
+                                 int inverse, const uint32_t *from,
                                  const uint32_t *to, size_t n_windows,
                                  int remove_mean, double *birkhoff_out,
                                  double *fft_out);
@@ -517,9 +551,9 @@ hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0,
  * is rejected with HM_ERR_INVALID_ARG.  The first call on each device looks
  * up the array's device address (cudaGetSymbolAddress); that lookup can
  * load the library's device code onto the device, which takes device
- * memory (the array itself among it), so make that first call -- or
- * hm_noalloc_prepare -- before the caller reserves its device memory and
- * before any stream capture.  The current device must own `stream` and the
+ * memory (the array itself among it), so make that first call (n = 0
+ * is enough) before the caller reserves its device memory and before any
+ * stream capture.  The current device must own `stream` and the
  * arrays; a stream of another device is rejected with HM_ERR_INVALID_ARG.
  * All calls on a device share the array: calls that overlap on the GPU
  * race.  Particle state after HM_ERR_TIMEOUT is as for hm_track_device.
@@ -531,12 +565,6 @@ hm_status hm_track_device_noalloc(double *x, double *px, double *y, double *py,
                                   uint32_t start_step, uint32_t n_turns,
                                   double mu, double barrier, int inverse,
                                   hm_arith arith, void *stream);
-/* No counterpart in the reference.  The set-up of hm_track_device_noalloc
- * for the current device, done ahead of time: it looks up the scratch
- * array's device address, loading the library's device code if it is not
- * loaded yet.  Call it once per device at start-up, before reserving device
- * memory; later calls return at once. */
-hm_status hm_noalloc_prepare(void);
 
 /* ---- device memory ----------------------------------------------------- */
 

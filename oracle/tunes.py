@@ -82,16 +82,23 @@ def tune_vec(x, px, y, py, frm, to, method: str):
     return out
 
 
-def orbit(x0, px0, y0, py0, tabs, n_turns, mu, barrier=10.0):
-    """Samples 0..n_turns of every particle: arrays [n_turns + 1][n]."""
+def orbit(x0, px0, y0, py0, tabs, n_turns, mu, barrier=10.0, kick_module=math.nan, seed=0,
+          inverse=False, steps0=None):
+    """Samples 0..n_turns of every particle: arrays [n_turns + 1][n].  With
+    kick_module, the reproducible kicks of (seed, particle index, table
+    index); with inverse, backward turns from steps0 (the particles' steps)."""
     n = len(np.atleast_1d(x0))
     cur = [np.array(np.atleast_1d(a), dtype=float) for a in (x0, px0, y0, py0)]
-    steps = np.zeros(n, np.uint32)
+    steps = np.zeros(n, np.uint32) if steps0 is None else np.array(steps0, dtype=np.uint32)
     out = np.empty((4, n_turns + 1, n))
     for c in range(4):
         out[c, 0] = cur[c]
     for k in range(n_turns):
-        x, px, y, py, steps = O.track(*cur, steps, tabs, 1, mu, barrier)
+        if math.isnan(kick_module):
+            x, px, y, py, steps = O.track(*cur, steps, tabs, 1, mu, barrier, inverse=inverse)
+        else:
+            x, px, y, py, steps = O.track_kicked(*cur, steps, tabs, 1, mu, barrier, kick_module,
+                                                 seed, inverse=inverse)
         cur = [x, px, y, py]
         for c in range(4):
             out[c, k + 1] = cur[c]

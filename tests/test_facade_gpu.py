@@ -197,3 +197,55 @@ def test_kicked_track_through_facade(gpu):
     np.testing.assert_array_equal(p.get_steps(), want[4])
     assert_bitwise(p.get_x(), want[0])
     assert_bitwise(p.get_py(), want[3])
+
+
+@pytest.mark.parametrize("every,n_steps,mu,dirs", [(10, 60, 0.2, ("x", "y")),
+                                                    (7, 700, 0.0, ("x", "py", "random")),
+                                                    (1, 300, 0.2, ("px",))])
+def test_fused_ghost_lyapunov_equals_the_loop(gpu, every, n_steps, mu, dirs):
+    # track_ghost_lyapunov against the notebook loop run on the reference's
+    # own GPU classes (or, without the reference build, on ours): the same
+    # coordinates and steps bit for bit -- lost bases, lost ghosts and ghosts
+    # of lost bases included -- and the same log sums to 1e-13.  700 steps
+    # of 7 turns cross the fused call's launch boundaries.
+    v = np.linspace(0, 0.6, 14)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    z = np.zeros_like(x)
+    module, eps = 1e-10, 64.0
+    turns = every * n_steps
+    p = hm.particles(x, z, y, z)
+    for d in dirs:
+        p.add_ghost(module, d)
+    t = hm.henon_tracker(turns + 1, 0.168, 0.201, "sps", np.nan, eps, 0)
+    got = t.track_ghost_lyapunov(p, n_steps, every, mu, module)
+    assert got.shape == (x.size, len(dirs))
+
+    R = O.reference_module("fmad_off")
+    if R is not None:
+        rp = R.particles_4d_gpu(x, z, y, z)
+        for d in dirs:
+            rp.add_ghost(module, d)
+        rt = R.henon_tracker_gpu(turns + 1, 0.168, 0.201, "sps", NAN, eps, 0)
+        step = lambda: rt.track(rp, every, mu, 10.0)  # noqa: E731
+    else:
+        rp = hm.particles(x, z, y, z)
+        for d in dirs:
+            rp.add_ghost(module, d)
+        rt = hm.henon_tracker(turns + 1, 0.168, 0.201, "sps", np.nan, eps, 0)
+        step = lambda: rt.track(rp, every, mu)  # noqa: E731
+    want = np.zeros((x.size, len(dirs)))
+    for _ in range(n_steps):
+        step()
+        want += np.log(np.asarray(rp.get_displacement_module()).reshape(x.size, len(dirs))
+                       / module)
+        rp.renormalize(module)
+    for name in ("get_x", "get_px", "get_y", "get_py"):
+        assert_bitwise(getattr(p, name)(), np.asarray(getattr(rp, name)()), name)
+    np.testing.assert_array_equal(p.get_steps(), np.asarray(rp.get_steps()))
+    assert np.array_equal(np.isnan(got), np.isnan(want))
+    m = ~np.isnan(want)
+    np.testing.assert_allclose(got[m], want[m], rtol=1e-13, atol=1e-12)
+    steps = p.get_steps()
+    assert np.any(steps[:x.size] < turns) and np.any(steps[:x.size] == turns)
+    assert p.particles.get_global_steps() == turns

@@ -502,7 +502,7 @@ def test_fast_mode_differences_lie_on_the_chaotic_border(gpu, eps, mu):
     v = C.Vectors(np.tile([1.0, 0.0, 0.0, 0.0], (x.size, 1)))
     ly = C.Lyapunov(x.size, [N])
     C.track_indicators(t, p, N, mu, 10.0, vectors=v, lyapunov=ly)
-    lyap = ly.get(False)[:, 0]
+    lyap = ly.get(False)[0]
     np.testing.assert_array_equal(p.get(C.FIELD_STEPS), exact[4])
     border = chaotic_border(side, exact[4], N, lyap, lam_c)
     surv_e, surv_f = exact[4] == N, fast[4] == N

@@ -137,3 +137,152 @@ def test_engine_get_tunes_matches_oracle(gpu):
     assert np.all(np.isnan(E.get_tunes(q, orb[1][:, 0])))
     with pytest.raises(RuntimeError, match="same size"):
         E.get_tunes(orb[0][:10, 0], orb[1][:9, 0])
+
+
+@pytest.mark.parametrize("kick,inverse", [(1e-6, False), (float("nan"), True), (1e-6, True)])
+def test_tracker_orbit_tunes_with_kicks_and_inverse(gpu, kick, inverse):
+    # birkhoff_tunes / all_tunes accept the reference's kick_module and
+    # inverse (src/henon.cu:2890-3078): the orbit is hm_track's (reproducible
+    # kicks keyed by kick_seed, particle and table index; backward turns from
+    # the particles' steps), then the same tunes.
+    x, px, y, py = grid(0.6, 9, px0=0.002)
+    n_fwd, n_turns, seed = 900, 600, 4242
+    frm, to = [0, 50], [99, 600]
+    tabs = O.tables(n_fwd, *TUNES, "sps", epsilon=16.0)
+    tr = C.Tracker(n_fwd, *TUNES, "sps", NAN, 16.0, 0)
+    p = C.Particles(x, px, y, py)
+    p.kick_seed = seed
+    start = (x, px, y, py, np.zeros(x.size, np.uint32))
+    if inverse:
+        tr.track(p, n_fwd, 0.2, 10.0)
+        start = O.track(x, px, y, py, start[4], tabs, n_fwd, 0.2, 10.0)
+    b, f = C.tracker_orbit_tunes(tr, p, n_turns, 0.2, 10.0, frm, to, True, True,
+                                 kick_module=kick, inverse=inverse)
+    orb = T.orbit(*start[:4], tabs, n_turns, 0.2, kick_module=kick, seed=seed, inverse=inverse,
+                  steps0=start[4])
+    got_state = p.state()
+    for c in range(4):
+        assert_bitwise(got_state[c], orb[c, -1], f"coordinate {c}")
+    assert p.global_steps == (n_fwd - n_turns if inverse else n_turns)
+    raw = orb
+    orb = T.remove_mean(orb)
+    want_b = np.array([T.tune_vec(*(orb[c, :, i] for c in range(4)), frm, to, "birkhoff")
+                       for i in range(x.size)])
+    want_f = np.array([T.tune_vec(*(orb[c, :, i] for c in range(4)), frm, to, "fft")
+                       for i in range(x.size)])
+    _close(b, want_b, 1e-13, "birkhoff")
+    _close(f, want_f, 1e-10, "fft")
+    # through the engine's reference-named methods too
+    from henon_map_cpp_b200 import henon_map_engine as E
+    et = E.henon_tracker_gpu(n_fwd, *TUNES, "sps", NAN, 16.0, 0)
+    ep = E.particles_4d_gpu(x, px, y, py)
+    ep.kick_seed = seed
+    if inverse:
+        et.track(ep, n_fwd, 0.2, 10.0)
+    eb = np.asarray(et.birkhoff_tunes(ep, n_turns, 0.2, 10.0, kick, inverse, frm, to))
+    want_raw = np.array([T.tune_vec(*(raw[c, :, i] for c in range(4)), frm, to, "birkhoff")
+                         for i in range(x.size)])
+    _close(eb[:, :2 * len(frm)], want_raw[:, :2 * len(frm)], 1e-13, "engine birkhoff_tunes")
+
+
+def test_tracker_megno_with_kicks_equals_construct_loop(gpu):
+    # megno(kick_module=...) (src/henon.cu:2755-2887 accepts kicks): the
+    # Jacobian of each turn at the point before it, then the kicked turn --
+    # the per-call loop with hm_track's reproducible kicks, bit for bit.
+    x, px, y, py = grid(0.5, 8)
+    n, kick, seed = x.size, 1e-7, 99
+    t = hm.henon_tracker(400, *TUNES, "sps", np.nan, 16.0, 0)
+    p = hm.particles(x, px, y, py)
+    p.particles.kick_seed = seed
+    got = t.megno(p, 400, 0.2, kick_module=kick, turn_samples=np.array([50, 400]))
+    t2 = hm.henon_tracker(400, *TUNES, "sps", np.nan, 16.0, 0)
+    p2 = hm.particles(x, px, y, py)
+    p2.particles.kick_seed = seed
+    M, Mo, mg = hm.matrix_4d_vector(n), hm.matrix_4d_vector(n), hm.megno_construct(n)
+    snaps = {}
+    for k in range(400):
+        Mo.explicit_copy(M)
+        M.structured_multiply(t2, p2, 0.2)
+        t2.track(p2, 1, 0.2, kick_module=kick)
+        mg.add(M, Mo)
+        if k + 1 in (50, 400):
+            snaps[k + 1] = mg.get_values()
+    assert_bitwise(got[:, 0], snaps[50])
+    assert_bitwise(got[:, 1], snaps[400])
+    assert_bitwise(p.get_x(), p2.get_x())
+    # without the kick the values differ (the kick is applied)
+    p3 = hm.particles(x, px, y, py)
+    plain = t.megno(p3, 400, 0.2, turn_samples=np.array([400]))
+    assert not np.array_equal(plain[:, 0], got[:, 1], equal_nan=True)
+
+
+def _inv_jacobian(x, px, y, py, sx, cx, sy, cy, mu):
+    """inverse_tangent_matrix (src/henon.cu:224-249) elementwise, [n][4][4]."""
+    u = cx * x - px * sx
+    w = cy * y - py * sy
+    d2 = u * u - w * w
+    gp = (3.0 * mu) * u + 1.0
+    gm = (-3.0 * mu) * u - 1.0
+    z = np.zeros_like(x)
+    m = np.empty((x.size, 4, 4))
+    rows = [[np.full_like(x, cx), np.full_like(x, -sx), z, z],
+            [(((-3.0 * cx) * mu) * d2 - (2.0 * cx) * u) + sx,
+             (cx + ((3.0 * mu) * sx) * d2) + (2.0 * sx) * u,
+             ((2.0 * cy) * w) * gp, ((2.0 * sy) * w) * gm],
+            [z, z, np.full_like(x, cy), np.full_like(x, -sy)],
+            [((2.0 * cx) * w) * gp, ((2.0 * sx) * w) * gm,
+             (((3.0 * cy) * mu) * d2 + (2.0 * cy) * u) + sy,
+             (cy - ((3.0 * mu) * sy) * d2) - (2.0 * sy) * u]]
+    for i in range(4):
+        for j in range(4):
+            m[:, i, j] = rows[i][j]
+    return m
+
+
+def test_tracker_megno_inverse_matches_oracle(gpu):
+    # megno(inverse=True): backward turns from the particles' steps, each
+    # with the Jacobian of the backward turn at the point before it; the
+    # MEGNO construct's accumulation (src/henon.cu:2253-2284).  Checked
+    # against a numpy restatement on the oracle's backward orbit (log10 of
+    # numpy against CUDA's: 1e-12).
+    x, px, y, py = grid(0.45, 7)
+    n, n_fwd, n_back, mu = x.size, 500, 300, 0.2
+    t = hm.henon_tracker(n_fwd, *TUNES, "sps", np.nan, 16.0, 0)
+    p = hm.particles(x, px, y, py)
+    t.track(p, n_fwd, mu)
+    got = t.megno(p, n_back, mu, inverse=True, turn_samples=np.array([100, 300]))
+    assert p.particles.get_global_steps() == n_fwd - n_back
+    sx, cx, sy, cy = O.tables(n_fwd, *TUNES, "sps", epsilon=16.0)
+    st = O.track(x, px, y, py, np.zeros(n, np.uint32), (sx, cx, sy, cy), n_fwd, mu, 10.0)
+    M = np.tile(np.eye(4), (n, 1, 1))
+    old = np.sqrt(np.sum(M.reshape(n, 16) ** 2, axis=1))
+    l1 = np.zeros(n)
+    l2 = np.zeros(n)
+    want = {}
+    s = n_fwd
+    with np.errstate(all="ignore"):
+        for k in range(1, n_back + 1):
+            s -= 1
+            J = _inv_jacobian(*st[:4], sx[s], cx[s], sy[s], cy[s], mu)
+            out = np.zeros_like(M)
+            for q in range(4):
+                out = out + J[:, :, q][:, :, None] * M[:, q, :][:, None, :]
+            M = out
+            sq = np.zeros(n)
+            for e in range(16):
+                sq = sq + M.reshape(n, 16)[:, e] ** 2
+            new = np.sqrt(sq)
+            lr = np.log10(new / old)
+            di = float(k)
+            l1 = l1 + lr * di
+            l2 = l2 + (1.0 / di) * l1
+            if k in (100, 300):
+                want[k] = (1.0 / di) * l2
+            old = new
+            st = O.track(*st, (sx, cx, sy, cy), 1, mu, 10.0, inverse=True)
+    for j, k in enumerate((100, 300)):
+        a, b = got[:, j], want[k]
+        assert np.array_equal(np.isnan(a), np.isnan(b))
+        m = ~np.isnan(b)
+        np.testing.assert_allclose(a[m], b[m], rtol=1e-12, atol=1e-14)
+    assert np.isfinite(got[:, 1]).any()

@@ -45,7 +45,6 @@ def test_noalloc_matches_allocating_entry_point_twice(gpu):
     trackers = [C.Tracker(n_turns, TUNES[0], TUNES[1], "sps", NAN, eps, 0) for eps in (64.0, 16.0)]
     ws = torch.empty(C.load().hm_track_workspace_bytes(n), dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    C.call("hm_noalloc_prepare")
     for call, (tr, mu) in enumerate(zip(trackers, (0.2, 0.0))):
         ref_c, ref_s = _device_state(torch, x, px, y, py)
         C.call("hm_track_device", *[c.data_ptr() for c in ref_c], ref_s.data_ptr(), n,
@@ -59,8 +58,8 @@ def test_noalloc_matches_allocating_entry_point_twice(gpu):
         torch.cuda.synchronize()
         free_after = torch.cuda.mem_get_info()[0]
         if call == 1:
-            # The set-up was done by hm_noalloc_prepare and the first call:
-            # the second takes no device memory at all.
+            # The first call did the per-device set-up; the second takes no
+            # device memory at all.
             assert free_after == free_before, (free_before, free_after)
         want, want_steps = _host(torch, ref_c, ref_s)
         have, have_steps = _host(torch, got_c, got_s)
