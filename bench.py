@@ -92,7 +92,6 @@ def workload_config(args, n_gpus):
             "particles_per_gpu": args.side * args.side, "turns": args.turns,
             "epsilon": list(EPSILONS), "mu": list(MUS), "tunes": list(TUNES),
             "arith": args.arith, "parallelism": f"particle shards x{n_gpus}",
-            "table_staging": args.stage_turns,
             "l2": "flushed between steps (256 MiB write); state < L2, compute-bound"}
 
 
@@ -256,17 +255,21 @@ def reference_cpu_sample(turns: int, side: int, repeats: int = 1, stride: int = 
 
 # ---- supplementary measurements (one GPU) ---------------------------------------------
 
-def bench_batched(C, arith):
+def bench_batched(C, arith, both_arith=True):
     """Mixed-size workload: 64 parameter sets, log-uniform 1k-256k particles
     in the 4D ball r < 0.6 and 1e3-1e6 turns, as one batch (graph replay)
-    versus one plain tracking call per set.  Survival counts must agree."""
+    versus one plain tracking call per set.  Survival counts must agree.
+    The batch runs the autotuner's shape for this GPU model and arithmetic
+    (autotune.batch_shape: the committed cache, or a tuning run); with
+    both_arith the other arithmetic is measured too, both arms in it."""
     import torch
 
-    from henon_map_cpp_b200 import sweep
+    from henon_map_cpp_b200 import autotune, sweep
 
     sets, coords = sweep.heterogeneous_sets(seed=20261203)
+    shape = autotune.batch_shape(sets, coords, arith)
     b = C.Batch(sets)
-    b.configure(arith, 1, 512, 4096)
+    autotune.configure_batch(b, shape, arith)
     b.load(*coords)
     b.run(True)  # capture + warm-up
     times = []
@@ -284,8 +287,7 @@ def bench_batched(C, arith):
     t0 = time.perf_counter()
     b.run(True)
     t_one_group = time.perf_counter() - t0
-    b.set_groups(16)
-    b.set_grid_share(1.5)
+    autotune.configure_batch(b, shape, arith)
     # plain: one chunked tracking call per set on device arrays
     t_plain, equal, o = 0.0, True, 0
     stream = torch.cuda.current_stream().cuda_stream
@@ -306,15 +308,23 @@ def bench_batched(C, arith):
         equal &= bool(np.array_equal(st.cpu().numpy().view(np.uint32), steps_batch[o:o + n]))
         o += n
     nominal = float(sum(s["n_particles"] * s["n_turns"] for s in sets))
-    return {"workload": "64 sets, tunes U[0.15,0.32], eps U[0,64], mu U[-0.5,0.5], "
-                        "log-uniform 1e3-2.56e5 particles in the 4D ball r<0.6, "
-                        "log-uniform 1e3-1e6 turns (seed 20261203)",
-            "particles": int(sum(s["n_particles"] for s in sets)),
-            "nominal_particle_turns": nominal, "executed_particle_turns": float(steps_batch.sum()),
-            "batched_s": t_batch, "one_group_s": t_one_group, "plain_sum_s": t_plain,
-            "speedup": t_plain / t_batch,
-            "batched_value": nominal / t_batch, "survival_equal_to_plain": equal,
-            "n_chunks": b.n_chunks(), "timing": "wall clock around synchronous runs, best of 2"}
+    out = {"workload": "64 sets, tunes U[0.15,0.32], eps U[0,64], mu U[-0.5,0.5], "
+                       "log-uniform 1e3-2.56e5 particles in the 4D ball r<0.6, "
+                       "log-uniform 1e3-1e6 turns (seed 20261203)",
+           "arith": "fast" if arith == C.ARITH_FAST else "exact",
+           "tuned_shape": shape, "shape_source": "autotune.batch_shape (tuning.json)",
+           "particles": int(sum(s["n_particles"] for s in sets)),
+           "nominal_particle_turns": nominal, "executed_particle_turns": float(steps_batch.sum()),
+           "batched_s": t_batch, "one_group_s": t_one_group, "plain_sum_s": t_plain,
+           "speedup": t_plain / t_batch,
+           "batched_value": nominal / t_batch, "survival_equal_to_plain": equal,
+           "n_chunks": b.n_chunks(), "timing": "wall clock around synchronous runs, best of 2"}
+    if both_arith:
+        other = C.ARITH_FAST if arith == C.ARITH_EXACT else C.ARITH_EXACT
+        o = bench_batched(C, other, both_arith=False)
+        out["other_arith"] = {k: o[k] for k in ("arith", "tuned_shape", "batched_s", "plain_sum_s",
+                                                  "speedup", "survival_equal_to_plain")}
+    return out
 
 
 def bench_long_horizon(C, arith, side=1024, turns=1_000_000):
@@ -393,8 +403,17 @@ def bench_adjoint(C):
             best = min(best, a.elapsed_time(b) * 1e-3)
         return best
 
-    t_adj = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100,
-                                          reverse="inverse"))
+    import ctypes
+
+    per_thread = {}
+    saved = ctypes.c_int()
+    C.call("hm_get_adjoint_config", ctypes.byref(saved))
+    for pt in (1, 2):
+        C.call("hm_set_adjoint_config", pt)
+        per_thread[pt] = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100,
+                                                       reverse="inverse"))
+    C.call("hm_set_adjoint_config", saved.value)
+    t_adj = per_thread[saved.value]
     t_replay = timed(lambda: AG.per_particle(*pts, theta, nt, checkpoint_every=100,
                                              reverse="replay"))
     t_loss = timed(lambda: AG.per_particle(*pts, theta, nt, mode="loss"))
@@ -414,7 +433,9 @@ def bench_adjoint(C):
     t_track = timed(track)
     r = AG.per_particle(*pts, theta, nt, checkpoint_every=100)
     return {"workload": "65,536 particles, 1e4 turns, eps 16, mu 0.1, checkpoints every 100",
-            "adjoint_s": t_adj, "adjoint_replay_s": t_replay, "forward_track_s": t_track,
+            "adjoint_s": t_adj, "adjoint_particles_per_thread": saved.value,
+            "adjoint_s_by_particles_per_thread": {str(k): v for k, v in per_thread.items()},
+            "adjoint_replay_s": t_replay, "forward_track_s": t_track,
             "forward_loss_s": t_loss, "adjoint_over_forward_track": t_adj / t_track,
             "reverse_sweep": "inverse map from the next checkpoint (replay variant also timed)",
             "survivors": int(r["survived"].sum().item()),
@@ -735,13 +756,18 @@ def run_ours(args):
     from henon_map_cpp_b200 import _capi as C  # fails loudly if the library is missing
 
     arith = C.ARITH_FAST if args.arith == "fast" else C.ARITH_EXACT
-    if args.stage_turns is not None:
-        C.set_track_staging(args.stage_turns)
-    args.stage_turns = C.get_track_staging()
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
 
     peak_tflops, _ = C.fp64_peak(0.3)
+    # Launch shape chosen by the autotuner for this GPU model and arithmetic
+    # (the committed tuning.json, or a tuning run of ~30 s when absent).
+    from henon_map_cpp_b200 import autotune
+
+    track_shape = autotune.apply(arith)
+    if args.stage_turns is not None:
+        C.set_track_staging(args.stage_turns)
+    args.stage_turns = C.get_track_staging()
 
     trackers = {eps: C.Tracker(args.turns, TUNES[0], TUNES[1], "sps", float("nan"), eps, 0)
                 for eps in EPSILONS}
@@ -983,6 +1009,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args, world),
             "rank_ms_per_step": rank_ms,
+            "track_shape": track_shape,
             "executed_particle_turns_per_s": executed / (total_ms * 1e-3),
             "survivor_fraction": executed / nominal,
             "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tflops,

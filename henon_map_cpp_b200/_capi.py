@@ -185,6 +185,8 @@ _SIGNATURES = {
                                    c_size_t, c_int, _PD]),
     # orbit-loss gradients
     "hm_adjoint_workspace_bytes": (c_size_t, [c_size_t, c_uint32, c_uint32]),
+    "hm_set_adjoint_config": (None, [c_int]),
+    "hm_get_adjoint_config": (None, [POINTER(c_int)]),
     "hm_adjoint": (None, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_double,
                           c_double, c_uint32, c_uint32, c_int, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_void_p, c_void_p, c_void_p]),

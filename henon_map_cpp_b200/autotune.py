@@ -10,11 +10,11 @@ are cached per GPU model and arithmetic in a JSON file next to this module
 (HENON_B200_TUNING overrides the path).
 
     from henon_map_cpp_b200 import autotune
-    autotune.apply()            # cached result, or tune now (~10-30 s)
+    autotune.apply()            # tracker shape: cached result, or tune now (~10-30 s)
+    autotune.configure_batch(batch, autotune.batch_shape(), arith)   # batched path
 """
 from __future__ import annotations
 
-import itertools
 import json
 import os
 import time
@@ -50,7 +50,9 @@ def _device_name() -> str:
     return torch.cuda.get_device_name()
 
 
-def _calibration(side: int = 512, turns: int = 20_000):
+def _calibration(side: int = 1024, turns: int = 20_000):
+    """The dynamic-aperture scan's grid (1024^2 on [0, 0.6]^2) over a shorter
+    horizon: the shapes are ranked on the workload they will run."""
     v = np.linspace(0.0, 0.6, side)
     xx, yy = np.meshgrid(v, v)
     x, y = xx.ravel(), yy.ravel()
@@ -116,27 +118,55 @@ def tune_track(arith: int = C.ARITH_EXACT, budget_s: float = 30.0, data=None):
     return cur, best, {str(k): v for k, v in timings.items()}
 
 
+BATCH_DEFAULT = {"groups": 16, "grid_share": 1.5, "per_thread": 1, "chunk0": 512,
+                 "chunk_max": 4096}
+
+
+def configure_batch(b, shape, arith: int) -> None:
+    """Applies a BATCH_SPACE shape to a C.Batch."""
+    b.set_groups(int(shape["groups"]))
+    b.set_grid_share(float(shape["grid_share"]))
+    b.configure(arith, int(shape["per_thread"]), int(shape["chunk0"]), int(shape["chunk_max"]))
+
+
 def tune_batch(sets, coords, arith: int = C.ARITH_EXACT, budget_s: float = 30.0):
-    """Grid search over BATCH_SPACE for one batch (wall time of a replay)."""
+    """Coordinate search over BATCH_SPACE from BATCH_DEFAULT for one batch
+    (wall time of a graph replay, best of two); returns (best shape, its
+    time in s, every timing)."""
     b = C.Batch(sets)
     b.load(*coords)
     res = {}
     start = time.perf_counter()
-    groups = None
-    for g, share, k, c0, cm in itertools.product(*BATCH_SPACE.values()):
-        if cm < c0 or time.perf_counter() - start > budget_s:
-            continue
-        if g != groups:
-            b.set_groups(g)
-            groups = g
-        b.set_grid_share(share)
-        b.configure(arith, k, c0, cm)
-        b.run(True)
-        t0 = time.perf_counter()
-        b.run(True)
-        res[(g, share, k, c0, cm)] = time.perf_counter() - t0
-    best = min(res, key=res.get)
-    return dict(zip(BATCH_SPACE, best)), res[best], {str(k): v for k, v in res.items()}
+
+    def cost(shape):
+        key = tuple(shape[k] for k in BATCH_SPACE)
+        if key not in res:
+            configure_batch(b, shape, arith)
+            b.run(True)  # capture + warm-up
+            best = float("inf")
+            for _ in range(2):
+                t0 = time.perf_counter()
+                b.run(True)
+                best = min(best, time.perf_counter() - t0)
+            res[key] = best
+        return res[key]
+
+    cur = dict(BATCH_DEFAULT)
+    best = cost(cur)
+    improved = True
+    while improved and time.perf_counter() - start < budget_s:
+        improved = False
+        for name, values in BATCH_SPACE.items():
+            for v in values:
+                if time.perf_counter() - start > budget_s:
+                    break
+                cand = dict(cur, **{name: v})
+                if cand["chunk_max"] < cand["chunk0"]:
+                    continue
+                c = cost(cand)
+                if c < best * 0.99:
+                    best, cur, improved = c, cand, True
+    return cur, best, {str(k): v for k, v in res.items()}
 
 
 def _load() -> dict:
@@ -146,18 +176,48 @@ def _load() -> dict:
         return {}
 
 
+def _key(arith: int) -> str:
+    return f"{_device_name()}|{'fast' if arith == C.ARITH_FAST else 'exact'}"
+
+
+def _store(key: str, entry: dict) -> None:
+    cache = _load()
+    cache.setdefault(key, {}).update(entry)
+    try:
+        CACHE.write_text(json.dumps(cache, indent=1, sort_keys=True) + "\n")
+    except OSError:
+        pass
+
+
+def batch_shape(sets=None, coords=None, arith: int = C.ARITH_EXACT, retune: bool = False,
+                budget_s: float = 60.0) -> dict:
+    """The batched path's shape for this GPU model and arithmetic from the
+    cache; tuned first (on `sets`/`coords`, default the mixed-size sweep of
+    sweep.heterogeneous_sets) when absent or when retune is set."""
+    key = _key(arith)
+    entry = _load().get(key, {})
+    if retune or "batch" not in entry:
+        if sets is None:
+            from .sweep import heterogeneous_sets  # noqa: PLC0415
+
+            sets, coords = heterogeneous_sets()
+        shape, secs, _ = tune_batch(sets, coords, arith, budget_s)
+        _store(key, {"batch": shape, "batch_s": secs,
+                     "batch_when": time.strftime("%Y-%m-%dT%H:%M:%S")})
+        return shape
+    return entry["batch"]
+
+
 def apply(arith: int = C.ARITH_EXACT, retune: bool = False, budget_s: float = 30.0) -> dict:
     """Sets the tracker's launch shape from the cache (tuning first when the
     GPU model/arithmetic has no entry or retune is set); returns it."""
-    key = f"{_device_name()}|{'fast' if arith == C.ARITH_FAST else 'exact'}"
-    cache = _load()
-    if retune or key not in cache:
-        shape, ms, timings = tune_track(arith, budget_s)
-        cache[key] = {"track": shape, "track_ms": ms, "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
-        try:
-            CACHE.write_text(json.dumps(cache, indent=1) + "\n")
-        except OSError:
-            pass
-    shape = cache[key]["track"]
+    key = _key(arith)
+    entry = _load().get(key, {})
+    if retune or "track" not in entry:
+        shape, ms, _ = tune_track(arith, budget_s)
+        _store(key, {"track": shape, "track_ms": ms,
+                     "when": time.strftime("%Y-%m-%dT%H:%M:%S")})
+        return shape
+    shape = entry["track"]
     _set_shape(shape)
     return shape

@@ -26,6 +26,19 @@ size_t hm_adjoint_workspace_bytes(size_t n, uint32_t n_turns, uint32_t checkpoin
                         sizeof(double));
 }
 
+hm_status hm_set_adjoint_config(int per_thread) {
+    if (per_thread != 1 && per_thread != 2)
+        return fail(HM_ERR_INVALID_ARG, "particles per thread must be 1 or 2");
+    hm::set_adjoint_per_thread(per_thread);
+    return ok();
+}
+
+hm_status hm_get_adjoint_config(int *per_thread) {
+    if (!per_thread) return fail(HM_ERR_INVALID_ARG, "null output");
+    *per_thread = hm::get_adjoint_per_thread();
+    return ok();
+}
+
 hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0, const double *y0,
                      const double *py0, size_t n, double mu, double barrier, uint32_t n_turns,
                      uint32_t checkpoint_every, int mode, double *loss, uint8_t *survived,

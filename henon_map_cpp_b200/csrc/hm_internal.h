@@ -356,6 +356,9 @@ struct AdjointArgs {
 // mode 0: loss + reverse-mode gradients; 1: loss + forward-mode initial-
 // condition gradient (tangent map); 2: loss only.
 cudaError_t launch_adjoint(const AdjointArgs &a, int mode, cudaStream_t s);
+// Particles per thread of the inverse-sweep adjoint kernel (1 or 2).
+void set_adjoint_per_thread(int p);
+int get_adjoint_per_thread();
 
 // ---- orbit tunes (tunes.cu / tunes.cpp) -----------------------------------------
 
@@ -408,9 +411,8 @@ struct BirkhoffSegArgs {
 cudaError_t launch_birkhoff_segments(const BirkhoffSegArgs &a, cudaStream_t s);
 
 // FFT tunes of one window of the tracker's orbit, both planes in one
-// batch: gather (mean removed, Hann window) into z[k][2n] (plane-major
-// columns, particles fastest), cuFFT, then one thread per column finds the
-// peak.
+// batch: gather (mean removed, Hann window) into rows z[plane n + i][k],
+// cuFFT, then one warp per row finds the peak.
 cudaError_t launch_hann_table(double *h, uint32_t len, cudaStream_t s);
 cudaError_t launch_fft_gather2(const double *x, const double *px, const double *y,
                                const double *py, const double *means, size_t n, uint32_t from,

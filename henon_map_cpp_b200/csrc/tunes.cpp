@@ -176,9 +176,9 @@ hm_status hm_orbit_tunes_host(const double *x, const double *px, const double *y
 namespace {
 
 // cuFFT plans of the tracker's tune path, kept across calls: one per
-// (device, length, batch), with the particle-fastest layout of
-// fft_gather2 (element k of column c at k * batch + c).  Creating a plan
-// costs more than running it at these sizes.
+// (device, length, batch), rows of `length` contiguous values (fft_gather2
+// writes both planes' rows, batch = 2 particles).  Creating a plan costs
+// more than running it at these sizes.
 struct PlanCache {
     std::mutex mutex;
     std::map<std::tuple<int, uint32_t, size_t>, cufftHandle> plans;
@@ -209,10 +209,9 @@ hm_status strided_plan(uint32_t len, size_t batch, cufftHandle *out) {
     }
     cufftHandle plan = 0;
     int nl = int(len);
-    const int stride = int(batch);
-    const cufftResult r = cufftPlanMany(&plan, 1, &nl, &nl, stride, 1, &nl, stride, 1, CUFFT_Z2Z,
+    const cufftResult r = cufftPlanMany(&plan, 1, &nl, nullptr, 1, nl, nullptr, 1, nl, CUFFT_Z2Z,
                                         int(batch));
-    if (r != CUFFT_SUCCESS) return cufft_fail(r, "strided plan");
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "plan");
     c.plans[key] = plan;
     *out = plan;
     return ok();

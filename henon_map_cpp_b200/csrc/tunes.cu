@@ -20,8 +20,8 @@
 // first NaN sample, and then never rewrites it: the mean is subtracted as
 // samples are read, Birkhoff sums run in segments of turns over many
 // threads (birkhoff_seg_kernel / birkhoff_finish_kernel), and the FFT
-// gather writes both planes of a window as one batch with particles
-// fastest (fft_gather2_kernel, fft_peak2_kernel).
+// gather writes both planes of a window as one batch of rows through
+// shared-memory tiles (fft_gather2_kernel, fft_peak2_kernel).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -108,6 +108,9 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
         a.sums[2 * n + i] = s2;
         a.sums[3 * n + i] = s3;
     }
+    // With the mean removed, one NaN sample makes the mean, and so every
+    // sample, NaN.
+    if (sums && first_nan <= a.n_turns) first_nan = 0u;
     if (a.first_nan) a.first_nan[i] = first_nan;
 }
 
@@ -208,55 +211,95 @@ __global__ void hann_table_kernel(double *h, uint32_t len) {
     h[k] = 2 * pow(s, 2);
 }
 
-// z[k][plane n + i] = ((q - mean) + i (p - mean)) h_k over the window's
-// samples from .. from + len - 1; consecutive threads take consecutive
-// particles (coalesced orbit reads and spectrum writes).
-__global__ void fft_gather2_kernel(const double *x, const double *px, const double *y,
-                                   const double *py, const double *means, size_t n,
-                                   uint32_t from, uint32_t len, const double *h, double2 *z,
-                                   size_t S) {
-    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const size_t cols = 2 * n;
-    if (t >= size_t(len) * cols) return;
-    const size_t k = t / cols, c = t - k * cols;
-    const int plane = c >= n ? 1 : 0;
-    const size_t i = c - size_t(plane) * n;
+// z[plane n + i][k] = ((q - mean) + i (p - mean)) h_k over the window's
+// samples from .. from + len - 1: one row of len values per column (plane,
+// particle), cuFFT's native batch layout.  A block moves a tile of 32
+// samples x 32 columns through shared memory, so that the orbit is read
+// along particles and the rows are written along samples, both coalesced.
+constexpr int kTile = 32;
+
+__global__ void __launch_bounds__(256) fft_gather2_kernel(const double *x, const double *px,
+                                                          const double *y, const double *py,
+                                                          const double *means, size_t n,
+                                                          uint32_t from, uint32_t len,
+                                                          const double *h, double2 *z, size_t S,
+                                                          int plane) {
+    __shared__ double2 tile[kTile][kTile + 1];
+    const size_t i0 = size_t(blockIdx.x) * kTile;  // first particle of the tile
+    const uint32_t k0 = blockIdx.y * kTile;        // first sample of the tile
     const double *q = plane ? y : x, *p = plane ? py : px;
-    const size_t o = size_t(from + k) * n + i;
-    const double re = centred(q[o], means, mean_of(means, n, i, 2 * plane, S));
-    const double im = centred(p[o], means, mean_of(means, n, i, 2 * plane + 1, S));
-    const double hk = h[k];
-    z[t] = make_double2(re * hk, im * hk);
+    const unsigned tx = threadIdx.x & 31u, ty = threadIdx.x >> 5;  // 8 warps
+    // read: lane tx takes particle i0 + tx; warp ty samples k0 + ty, + 8, ...
+    {
+        const size_t i = i0 + tx;
+        const bool ok_i = i < n;
+        const double mq = ok_i ? mean_of(means, n, i, 2 * plane, S) : 0.0;
+        const double mp = ok_i ? mean_of(means, n, i, 2 * plane + 1, S) : 0.0;
+        for (unsigned r = ty; r < unsigned(kTile); r += 8u) {
+            const uint32_t k = k0 + r;
+            double2 v = make_double2(0.0, 0.0);
+            if (ok_i && k < len) {
+                const size_t o = size_t(from + k) * n + i;
+                const double re = centred(q[o], means, mq), im = centred(p[o], means, mp);
+                const double hk = h[k];
+                v = make_double2(re * hk, im * hk);
+            }
+            tile[r][tx] = v;
+        }
+    }
+    __syncthreads();
+    // write: warp ty takes particles i0 + ty, + 8, ...; lane tx sample k0 + tx
+    for (unsigned ii = ty; ii < unsigned(kTile); ii += 8u) {
+        const size_t i = i0 + ii;
+        const uint32_t k = k0 + tx;
+        if (i < n && k < len) z[(size_t(plane) * n + i) * len + k] = tile[tx][ii];
+    }
 }
 
-// One thread per column (plane, particle): first maximum of |z_k| over k,
-// then the interpolation of src/dynamic_indicator.cpp:139-176 -> |1 - v|;
-// NaN when the window's samples from .. last_sample hold a NaN.
+// One warp per column (plane, particle): first maximum of |z_k| over k
+// (lanes stride the row, then a shuffle reduction keeping the smallest k
+// among equal maxima), then the interpolation of
+// src/dynamic_indicator.cpp:139-176 -> |1 - v|; NaN when the window's
+// samples from .. last_sample hold a NaN.
 __global__ void fft_peak2_kernel(const double2 *z, uint32_t len, size_t n, uint32_t last_sample,
                                  const uint32_t *first_nan, double *out, size_t out_cols,
                                  int col) {
-    const size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const size_t cols = 2 * n;
-    if (c >= cols) return;
+    const size_t c = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const unsigned lane = threadIdx.x & 31u;
+    if (c >= 2 * n) return;
     const int plane = c >= n ? 1 : 0;
     const size_t i = c - size_t(plane) * n;
+    const double2 *row = z + c * len;
     auto mag = [&](uint32_t k) {
-        const double2 v = z[size_t(k) * cols + c];
+        const double2 v = row[k];
         return sqrt(v.x * v.x + v.y * v.y);
     };
-    double value;
-    if (first_nan[i] <= last_sample) {
-        value = dev::quiet_nan();
-    } else {
-        double best = -1.0;
-        uint32_t index = 0;
-        for (uint32_t k = 0; k < len; ++k) {
+    const bool nan = first_nan[i] <= last_sample;
+    double best = -1.0;
+    uint32_t best_k = 0xffffffffu;
+    if (!nan) {
+        for (uint32_t k = lane; k < len; k += 32) {
             const double m = mag(k);
-            if (m > best) {
+            if (m > best) {  // k grows within a lane: the first maximum is kept
                 best = m;
-                index = k;
+                best_k = k;
             }
         }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(dev::kFullMask, best, o);
+        const uint32_t ok = __shfl_down_sync(dev::kFullMask, best_k, o);
+        if (ob > best || (ob == best && ok < best_k)) {
+            best = ob;
+            best_k = ok;
+        }
+    }
+    if (lane != 0) return;
+    double value;
+    if (nan) {
+        value = dev::quiet_nan();
+    } else {
+        uint32_t index = best_k;
         const double N = double(len);
         if (index == 0) {
             value = 1.0;
@@ -493,18 +536,22 @@ cudaError_t launch_fft_gather2(const double *x, const double *px, const double *
                                const double *py, const double *means, size_t n, uint32_t from,
                                uint32_t len, const double *h, double2 *z, size_t S,
                                cudaStream_t s) {
-    const size_t total = size_t(len) * 2 * n;
-    if (total == 0) return cudaSuccess;
-    fft_gather2_kernel<<<unsigned((total + 255) / 256), 256, 0, s>>>(x, px, y, py, means, n,
-                                                                      from, len, h, z, S);
-    return cudaGetLastError();
+    if (n == 0 || len == 0) return cudaSuccess;
+    const dim3 grid(unsigned((n + kTile - 1) / kTile), (len + kTile - 1) / kTile);
+    for (int plane = 0; plane < 2; ++plane) {
+        fft_gather2_kernel<<<grid, 256, 0, s>>>(x, px, y, py, means, n, from, len, h, z, S, plane);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_fft_peak2(const double2 *z, uint32_t len, size_t n, uint32_t last_sample,
                              const uint32_t *first_nan, double *out, size_t cols, int col,
                              cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    fft_peak2_kernel<<<unsigned((2 * n + 127) / 128), 128, 0, s>>>(z, len, n, last_sample,
+    const size_t threads = 2 * n * 32;
+    fft_peak2_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(z, len, n, last_sample,
                                                                     first_nan, out, cols, col);
     return cudaGetLastError();
 }

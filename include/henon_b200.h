@@ -533,6 +533,10 @@ hm_status hm_storage_tunes(const hm_storage *s, const uint32_t *from,
  * Derivatives need an "sps" or "basic" modulation.  Synchronous. */
 size_t hm_adjoint_workspace_bytes(size_t n, uint32_t n_turns,
                                   uint32_t checkpoint_every);
+/* Particles per thread of mode 3's kernel (1 or 2).  Process-wide; chosen
+ * by the autotuner; results do not depend on it. */
+hm_status hm_set_adjoint_config(int per_thread);
+hm_status hm_get_adjoint_config(int *per_thread);
 hm_status hm_adjoint(const hm_tracker *t, const double *x0, const double *px0,
                      const double *y0, const double *py0, size_t n, double mu,
                      double barrier, uint32_t n_turns, uint32_t checkpoint_every,
