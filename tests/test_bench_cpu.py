@@ -83,6 +83,6 @@ def test_cpu_sample_is_fixed():
     # same fixed stride of the grid.
     import inspect
 
-    assert bench.CPU_STRIDE == 16
+    assert bench.CPU_STRIDE == 24
     sig = inspect.signature(bench.reference_cpu_sample)
     assert sig.parameters["stride"].default == bench.CPU_STRIDE
