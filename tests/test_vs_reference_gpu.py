@@ -93,3 +93,61 @@ def test_faster_than_reference_gpu_path(gpu):
     # sea may differ; the stable core must agree.
     assert abs(ref["survivors"] - survivors) <= 0.01 * n
     assert our_rate > 3.0 * ref_rate
+
+
+_TUNES_CHILD = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from oracle import oracle as O
+d = np.load(sys.argv[2])
+R = O.reference_module("default")
+t = R.henon_tracker(int(d["n_turns"]), float(d["tunes"][0]), float(d["tunes"][1]), "sps",
+                    float("nan"), float(d["epsilon"]), 0)
+frm, to = [int(v) for v in d["frm"]], [int(v) for v in d["to"]]
+p = R.particles_4d(d["x"], d["px"], d["y"], d["py"])
+b = np.asarray(t.birkhoff_tunes(p, int(d["n_turns"]), float(d["mu"]), 10.0, float("nan"), False,
+                                frm, to))
+p = R.particles_4d(d["x"], d["px"], d["y"], d["py"])
+ab, af = t.all_tunes(p, int(d["n_turns"]), float(d["mu"]), 10.0, float("nan"), False, frm, to)
+np.savez(sys.argv[3], birkhoff=b, all_birkhoff=np.asarray(ab), all_fft=np.asarray(af))
+"""
+
+
+@pytest.mark.skipif(not (O.REF_DIR / "default").exists(), reason="reference build absent")
+def test_tunes_match_the_reference_cpu_tracker(gpu, tmp_path):
+    # birkhoff_tunes and all_tunes of the reference's own henon_tracker
+    # (src/henon.cu:2890-3078: CPU tracking, Birkhoff sums, FFTW tunes --
+    # cuFFTW in the checker build) against ours on the same particles.
+    # Birkhoff: 1e-13 (our sums run in segments of turns); FFT: 1e-10.
+    from henon_map_cpp_b200 import henon_map_engine as E
+
+    x, px, y, py = (np.ascontiguousarray(a) for a in _grid_small())
+    n_turns, eps, mu = 2000, 16.0, 0.2
+    frm, to = [0, 100, 700], [500, 1001, 1999]
+    inp, out = tmp_path / "in.npz", tmp_path / "out.npz"
+    np.savez(inp, x=x, px=px, y=y, py=py, n_turns=n_turns, tunes=np.asarray(TUNES),
+             epsilon=eps, mu=mu, frm=np.asarray(frm), to=np.asarray(to))
+    subprocess.run([sys.executable, "-c", _TUNES_CHILD, str(REPO), str(inp), str(out)],
+                   check=True, capture_output=True, text=True)
+    ref = np.load(out)
+    t = E.henon_tracker_gpu(n_turns, TUNES[0], TUNES[1], "sps", NAN, eps, 0)
+    b = np.asarray(t.birkhoff_tunes(E.particles_4d_gpu(x, px, y, py), n_turns, mu, 10.0, NAN,
+                                    False, frm, to))
+    ab, af = (np.asarray(a) for a in t.all_tunes(E.particles_4d_gpu(x, px, y, py), n_turns, mu,
+                                                  10.0, NAN, False, frm, to))
+    for got, want, rtol, what in ((b, ref["birkhoff"], 1e-13, "birkhoff_tunes"),
+                                  (ab, ref["all_birkhoff"], 1e-13, "all_tunes birkhoff"),
+                                  (af, ref["all_fft"], 1e-10, "all_tunes fft")):
+        assert got.shape == want.shape, what
+        assert np.array_equal(np.isnan(got), np.isnan(want)), what
+        m = ~np.isnan(want)
+        np.testing.assert_allclose(got[m], want[m], rtol=rtol, atol=1e-14, err_msg=what)
+    assert np.isnan(ab).any() and np.isfinite(af).any()
+
+
+def _grid_small():
+    v = np.linspace(0.0, 0.55, 12)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    return x, np.full_like(x, 0.001), y, np.zeros_like(y)
