@@ -39,22 +39,33 @@ using dev::Particle;
 constexpr uint32_t kStageTurns = 32u;
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
-constexpr int kPerLane = int(kStageTurns) * 4 / 32;
 
-// Records [lo, lo + kn) of a table; element e of the stage = table[4 lo + e].
-__device__ __forceinline__ void stage_load(double (&r)[kPerLane], const double *table, uint32_t lo,
-                                           uint32_t kn, unsigned lane) {
+// Records [lo, lo + kn) of a table into a warp's stage buffer with
+// asynchronous 16-byte copies (cp.async, no registers held): chunk c of the
+// stage (two doubles) is table[4 lo + 2c ..]; chunks past the kn records
+// are zero-filled without reading.  Sources are 16-byte aligned (32-byte
+// records of a 256-byte-aligned table), and so is the buffer.
+constexpr int kChunksPerLane = int(kStageTurns) * 4 / 2 / 32;
+static_assert(kChunksPerLane * 32 * 2 == int(kStageTurns) * 4, "stage must split evenly");
+
+__device__ __forceinline__ void stage_async(double *buf, const double *table, uint32_t lo,
+                                            uint32_t kn, unsigned lane) {
 #pragma unroll
-    for (int q = 0; q < kPerLane; ++q) {
-        const uint32_t e = lane + 32u * uint32_t(q);
-        r[q] = e < 4u * kn ? __ldg(table + 4u * size_t(lo) + e) : 0.0;
+    for (int q = 0; q < kChunksPerLane; ++q) {
+        const uint32_t c = lane + 32u * uint32_t(q);
+        const bool in = c < 2u * kn;
+        const double *src = table + (in ? 4u * size_t(lo) + 2u * c : 0u);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dev::smem_addr(buf + 2u * c)),
+                     "l"(src), "r"(in ? 16u : 0u)
+                     : "memory");
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-__device__ __forceinline__ void stage_store(double *buf, const double (&r)[kPerLane],
-                                            unsigned lane) {
-#pragma unroll
-    for (int q = 0; q < kPerLane; ++q) buf[lane + 32u * uint32_t(q)] = r[q];
+// This lane's copies have landed; with the __syncwarp after it, every
+// lane's.
+__device__ __forceinline__ void stage_wait() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 // Copies every non-NaN particle of every set into list 0 of its set and
@@ -115,16 +126,20 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
                                          const BatchStateDev &st, uint32_t s, uint32_t start,
                                          int in, int out, double *bufs, double2 *ckpt) {
     const unsigned lane = threadIdx.x & 31u;
+    // A particle's slot in the input list is recomputed from the tile, and
+    // its 64-bit index read back from the list only when it is written out
+    // (lost, final chunk) or appended to the next list: fewer registers.
+    auto slot_of = [&](int j) {
+        return set.list_offset + start + uint32_t(j) * 32u + lane;
+    };
     Particle p[K];
-    uint64_t id[K];
     bool live[K];
     bool any = false;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
         const uint32_t e = start + uint32_t(j) * 32u + lane;
         live[j] = e < st.live;
-        const uint64_t slot = set.list_offset + (live[j] ? e : 0u);
-        id[j] = b.list_idx[in][slot];
+        const uint64_t slot = live[j] ? slot_of(j) : set.list_offset;
         p[j] = dev::make_particle(b.list_x[in][slot], b.list_px[in][slot], b.list_y[in][slot],
                                   b.list_py[in][slot]);
         // Slots without a live particle hold zeros, a fixed point of the map.
@@ -133,21 +148,22 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
     }
     const uint32_t turn0 = st.done, nt = st.turns;
     const double mu = set.mu;
-    const dev::Barrier bar = dev::make_barrier<ARITH>(set.b2bits);
+    // The common path needs only the coordinate bound of the barrier test;
+    // the rare per-turn redo rebuilds the whole test from b2bits.
+    const uint32_t small_hi = dev::make_barrier<ARITH>(set.b2bits).small_hi;
     bool warp_live = __any_sync(dev::kFullMask, any);
     const uint32_t n_stages = (nt + kStageTurns - 1) / kStageTurns;
-    double next[kPerLane];
-    if (warp_live && n_stages > 0) {
-        stage_load(next, set.table, turn0, min(kStageTurns, nt), lane);
-        stage_store(bufs, next, lane);
-    }
+    if (warp_live && n_stages > 0) stage_async(bufs, set.table, turn0, min(kStageTurns, nt), lane);
+    stage_wait();
     __syncwarp();
     for (uint32_t sg = 0; warp_live && sg < n_stages; ++sg) {
         const uint32_t k0 = sg * kStageTurns, kn_stage = min(kStageTurns, nt - k0);
         const bool more = sg + 1 < n_stages;
+        // The other buffer was last read in the previous stage, which every
+        // lane has finished.
         if (more)
-            stage_load(next, set.table, turn0 + k0 + kStageTurns,
-                       min(kStageTurns, nt - k0 - kStageTurns), lane);
+            stage_async(bufs + ((sg + 1u) & 1u) * kStageTurns * 4u, set.table,
+                        turn0 + k0 + kStageTurns, min(kStageTurns, nt - k0 - kStageTurns), lane);
         const double *rec = bufs + (sg & 1u) * kStageTurns * 4u;
         // The stage's turns with no per-turn control flow, ORing every
         // coordinate's high word; one vote at the end.  Only a warp with a
@@ -170,7 +186,9 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
                 ored_stage |= dev::hi_or(p[j]);
             }
         }
-        const bool redo = __any_sync(dev::kFullMask, !dev::small_or(ored_stage, bar));
+        // (small_or with the bound alone: the OR of the high words, sign
+        // masked, against the coordinate bound)
+        const bool redo = __any_sync(dev::kFullMask, (ored_stage & 0x7fffffffu) >= small_hi);
         if (redo) {
 #pragma unroll
             for (int j = 0; j < K; ++j) {
@@ -179,6 +197,7 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
                 p[j] = dev::make_particle(a.x, a.y, c.x, c.y);
             }
         }
+        const dev::Barrier bar = dev::make_barrier<ARITH>(set.b2bits);
         for (uint32_t kk = 0; redo && warp_live && kk < kn_stage; ++kk) {
             const uint32_t k = k0 + kk;
             const double2 *q = reinterpret_cast<const double2 *>(rec + 4u * kk);
@@ -198,8 +217,9 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
                 for (int j = 0; j < K; ++j) {
                     if (live[j] && !dev::small_inside(p[j], bar) &&
                         !dev::inside<ARITH>(dev::radius_fma(p[j]), p[j], bar)) {
-                        b.x[id[j]] = b.px[id[j]] = b.y[id[j]] = b.py[id[j]] = dev::quiet_nan();
-                        b.steps[id[j]] = turn0 + k;
+                        const uint64_t id = b.list_idx[in][slot_of(j)];
+                        b.x[id] = b.px[id] = b.y[id] = b.py[id] = dev::quiet_nan();
+                        b.steps[id] = turn0 + k;
                         live[j] = false;
                         p[j] = dev::make_particle(0.0, 0.0, 0.0, 0.0);
                     }
@@ -208,21 +228,25 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
                 warp_live = __any_sync(dev::kFullMask, still);
             }
         }
-        // The other buffer was last read in the previous stage, which every
-        // lane has finished.
-        if (more) stage_store(bufs + ((sg + 1u) & 1u) * kStageTurns * 4u, next, lane);
+        // The next stage's copies have landed.
+        stage_wait();
         __syncwarp();
     }
+    // No copy may still be in flight when the warp moves to its next tile
+    // (a stage left early by an all-lost warp).
+    stage_wait();
+    __syncwarp();
     const bool final_chunk = turn0 + nt == set.n_turns;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
         if (final_chunk) {
             if (live[j]) {
-                b.x[id[j]] = p[j].x;
-                b.px[id[j]] = p[j].px;
-                b.y[id[j]] = p[j].y;
-                b.py[id[j]] = p[j].py;
-                b.steps[id[j]] = set.n_turns;
+                const uint64_t id = b.list_idx[in][slot_of(j)];
+                b.x[id] = p[j].x;
+                b.px[id] = p[j].px;
+                b.y[id] = p[j].y;
+                b.py[id] = p[j].py;
+                b.steps[id] = set.n_turns;
             }
             continue;
         }
@@ -234,7 +258,7 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
         off = __shfl_sync(dev::kFullMask, off, leader);
         if (live[j]) {
             const uint64_t slot = set.list_offset + off + __popc(m & ((1u << lane) - 1u));
-            b.list_idx[out][slot] = id[j];
+            b.list_idx[out][slot] = b.list_idx[in][slot_of(j)];
             b.list_x[out][slot] = p[j].x;
             b.list_px[out][slot] = p[j].px;
             b.list_y[out][slot] = p[j].y;
@@ -243,10 +267,14 @@ __device__ __forceinline__ void run_tile(const BatchDev &b, const BatchSetDev &s
     }
 }
 
-// Persistent: warps pop warp-tiles until the chunk's queue is empty.  One
-// particle per thread fits 72 registers without spills: 7 blocks per SM.
+// Persistent: warps pop warp-tiles until the chunk's queue is empty.  With
+// the turn records copied by cp.async (no staging registers), particle
+// slots recomputed from the tile and only the barrier's coordinate bound in
+// registers, one particle per thread fits 64 registers (8 blocks per SM)
+// and two fit 90 (5 blocks per SM).
 template <int ARITH, int K>
-__global__ void __launch_bounds__(kThreads, K == 1 ? 7 : 1) batch_chunk_kernel(BatchDev b) {
+__global__ void __launch_bounds__(kThreads, K == 1 ? 8 : (K == 2 ? 5 : 1))
+    batch_chunk_kernel(BatchDev b) {
     __shared__ __align__(16) double stage_bufs[kWarps][2 * kStageTurns * 4];
     // Per warp, the particles {x, px}, {y, py} at the start of a stage.
     __shared__ __align__(16) double2 checkpoints[kWarps][2 * 32 * K];

@@ -115,9 +115,13 @@ __global__ void __launch_bounds__(128) ghost_lyapunov_kernel(const GhostLyapunov
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     const double mu = a.mu, module = a.module;
     uint32_t turn = a.turn0;
+    const uint32_t end = a.turn0 + a.n_steps * a.every;
+    // The next turn's record is loaded a turn ahead, off the orbits' chains.
+    dev::Turn t_next = a.n_steps ? dev::load_turn(a.table, turn) : dev::Turn{};
     for (uint32_t st = 0; st < a.n_steps; ++st) {
         for (uint32_t k = 0; k < a.every; ++k, ++turn) {
-            const dev::Turn t = dev::load_turn(a.table, turn);
+            const dev::Turn t = t_next;
+            if (turn + 1 < end) t_next = dev::load_turn(a.table, turn + 1);
             uint32_t ored = 0u;
 #pragma unroll
             for (int j = 0; j < K; ++j) {

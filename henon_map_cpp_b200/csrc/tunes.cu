@@ -65,12 +65,17 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
     dev::Particle p = dev::make_particle(x, px, y, py);
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     const unsigned long long id = a.id0 + i;
+    // The next turn's record is loaded a turn ahead, off the orbit's chain.
+    auto table_index = [&](uint32_t k) { return REV ? a.live_step - 1u - k : a.live_step + k; };
+    dev::Turn t_next = a.n_turns ? dev::load_turn(a.table, table_index(0)) : dev::Turn{};
     for (uint32_t k = 0; k < a.n_turns; ++k) {
+        const dev::Turn t = t_next;
+        if (k + 1 < a.n_turns) t_next = dev::load_turn(a.table, table_index(k + 1));
         if (alive) {
-            const uint32_t idx = REV ? a.live_step - 1u - k : a.live_step + k;
+            const uint32_t idx = table_index(k);
             if (KICK && !REV)
                 dev::apply_kick<false>(p, dev::kick_direction(a.kick_seed, id, idx), a.kick_module);
-            dev::turn<ARITH, OCT, REV>(p, dev::load_turn(a.table, idx), a.mu);
+            dev::turn<ARITH, OCT, REV>(p, t, a.mu);
             if (KICK && REV)
                 dev::apply_kick<true>(p, dev::kick_direction(a.kick_seed, id, idx), a.kick_module);
             if (dev::inside_after_turn<ARITH>(p, bar)) {

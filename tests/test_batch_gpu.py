@@ -36,12 +36,14 @@ def test_batch_equals_plain_per_set(gpu, arith):
     res_graph = sweep.run_sweep(sets, coords, arith=arith, chunk0=64, chunk_max=1024)
     res_plain = sweep.run_sweep(sets, coords, arith=arith, chunk0=100, chunk_max=100,
                                 per_thread=4, use_graph=False)
+    res_two = sweep.run_sweep(sets, coords, arith=arith, chunk0=128, chunk_max=2048,
+                              per_thread=2)
     o = 0
-    for s, rg, rp in zip(sets, res_graph, res_plain):
+    for s, rg, rp, r2 in zip(sets, res_graph, res_plain, res_two):
         n = s["n_particles"]
         want = plain(s, *(c[o:o + n] for c in coords), arith)
         o += n
-        for r in (rg, rp):
+        for r in (rg, rp, r2):
             np.testing.assert_array_equal(r["steps"], want[4])
             for k, w in zip(("x", "px", "y", "py"), want[:4]):
                 assert_bitwise(r[k], w, k)

@@ -140,10 +140,25 @@ def test_tunes_match_the_reference_cpu_tracker(gpu, tmp_path):
                                   (ab, ref["all_birkhoff"], 1e-13, "all_tunes birkhoff"),
                                   (af, ref["all_fft"], 1e-10, "all_tunes fft")):
         assert got.shape == want.shape, what
-        assert np.array_equal(np.isnan(got), np.isnan(want)), what
+        if what == "all_tunes fft":
+            # The reference's NaN scan of a window reads from the window's
+            # start to past the end of the orbit vector
+            # (src/dynamic_indicator.cpp:284-287), so it may report NaN for a
+            # window without one; here the window itself is scanned.  Where
+            # the reference gives a value, ours must match it; the full
+            # orbit (its last two columns) is scanned correctly by both.
+            full = slice(-2, None)
+            assert np.array_equal(np.isnan(got[:, full]), np.isnan(want[:, full])), what
+            assert np.all(np.isnan(got) <= np.isnan(want)), what
+        else:
+            assert np.array_equal(np.isnan(got), np.isnan(want)), what
         m = ~np.isnan(want)
         np.testing.assert_allclose(got[m], want[m], rtol=rtol, atol=1e-14, err_msg=what)
     assert np.isnan(ab).any() and np.isfinite(af).any()
+    # the window scan: a window of a particle that survives all turns is
+    # finite here whatever the reference's scan past the vector end found
+    alive = np.all(np.isfinite(ab), axis=1)
+    assert np.all(np.isfinite(af[alive]))
 
 
 def _grid_small():
