@@ -29,6 +29,52 @@ namespace {
 
 using dev::Rn;
 
+// The windows of one kind that still take samples at sample index idx,
+// as a bit set over the window slots (at most 64 windows per kind; more fall
+// back to testing every window every turn).  Window w is open while
+// idx < limit_w (limit = T + 1 for MEGNO-Birkhoff, the length for
+// Lyapunov, twice the length for the tunes' two windows); `next` is the
+// first index at which an open window closes, when the set is rebuilt.
+// Per turn a warp then visits only its open windows instead of loading
+// and comparing every window's bound.
+struct OpenWindows {
+    uint64_t mask = 0, next = ~0ull;
+};
+
+template <int KIND>  // 0: MEGNO-Birkhoff (T), 1: Lyapunov (length), 2: tunes (2 length)
+__device__ __forceinline__ uint64_t window_limit(const uint64_t *bound, int w) {
+    const uint64_t b = bound[w];
+    return KIND == 0 ? b + 1u : (KIND == 1 ? b : 2u * b);
+}
+
+template <int KIND>
+__device__ __forceinline__ void open_windows(OpenWindows &o, const uint64_t *bound, int n,
+                                             uint64_t idx) {
+    if (n > 64) {  // every window is tested every turn
+        o.next = ~0ull;
+        return;
+    }
+    o.mask = 0;
+    o.next = ~0ull;
+    for (int w = 0; w < n; ++w) {
+        const uint64_t lim = window_limit<KIND>(bound, w);
+        if (idx < lim) {
+            o.mask |= 1ull << w;
+            o.next = lim < o.next ? lim : o.next;
+        }
+    }
+}
+
+// Next sample turn of MEGNO at or after idx (~0 when none).
+__device__ __forceinline__ uint64_t next_sample(const uint64_t *turns, int n, uint64_t idx) {
+    uint64_t best = ~0ull;
+    for (int j = 0; j < n; ++j) {
+        const uint64_t s = turns[j];
+        if (s >= idx && s < best) best = s;
+    }
+    return best;
+}
+
 // SPLIT: every particle is followed by two warps.  Both track it (the
 // same operations, so the same orbit); the even warp of a pair also carries
 // the tangent matrix, MEGNO and the MEGNO-Birkhoff windows, the odd one the
@@ -107,6 +153,21 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
     const double mu = a.mu;
     const dev::Barrier bar = dev::make_barrier<HM_ARITH_EXACT>(a.b2bits);
     bool warp_live = __any_sync(dev::kFullMask, alive);
+    // Two open-window sets per thread (registers): a thread with the matrix
+    // work keeps its MEGNO-Birkhoff windows in the first and its next MEGNO
+    // sample turn in the second's `next`; a thread with the vector or tune
+    // work its Lyapunov windows in the first and its tune windows in the
+    // second.  No thread has both (the matrix work is split from the others
+    // whenever both are asked for), and a kind left without a set tests
+    // every window every turn.
+    const bool snap_in_b = do_m && a.megno_l1 && a.n_snap > 0;
+    const bool all_mb = a.n_mb > 64, all_ly = a.n_ly > 64 || (do_m && a.mb_l1),
+               all_tu = a.n_tu > 64 || snap_in_b;
+    OpenWindows setA, setB;
+    if (do_m && a.mb_l1 && !all_mb) open_windows<0>(setA, a.mb_T, a.n_mb, a.mb_idx);
+    else if (do_v && a.n_ly && !all_ly) open_windows<1>(setA, a.ly_len, a.n_ly, a.ly_idx);
+    if (snap_in_b) setB.next = next_sample(a.snap_turns, a.n_snap, a.megno_idx);
+    else if (do_t && !all_tu) open_windows<2>(setB, a.tu_T, a.n_tu, a.tu_idx);
     uint32_t k = 0;
     for (; k < a.n_turns && warp_live; ++k) {
         double df[16];
@@ -171,19 +232,32 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
                 m_l1 = Rn::add(m_l1, Rn::mul(lr, di));
                 m_l2 = Rn::add(m_l2, Rn::mul(inv, m_l1));
                 m_l3 = Rn::mul(inv, m_l2);
-                for (int j = 0; j < a.n_snap; ++j)
-                    if (a.snap_turns[j] == a.megno_idx + k && in_range)
-                        a.snap[size_t(j) * n + ii] = m_l3;
+                const uint64_t cur = a.megno_idx + k;
+                if (snap_in_b && cur == setB.next) {  // a sample turn: every slot that asks
+                    for (int j = 0; j < a.n_snap; ++j)
+                        if (a.snap_turns[j] == cur && in_range) a.snap[size_t(j) * n + ii] = m_l3;
+                    setB.next = next_sample(a.snap_turns, a.n_snap, cur + 1u);
+                }
             }
             if (a.mb_l1) {
                 const uint64_t idx = a.mb_idx + k;
                 const double di = double(idx);
                 b_l1 = Rn::add(b_l1, Rn::mul(lr, di));
-                for (int w = 0; w < a.n_mb; ++w)
-                    if (idx <= a.mb_T[w]) {
+                if (all_mb) {
+                    for (int w = 0; w < a.n_mb; ++w)
+                        if (idx <= a.mb_T[w]) {
+                            double &acc = mb_l2[w * T + tid];
+                            acc = Rn::add(acc,
+                                          Rn::div(Rn::mul(b_l1, a.mb_w[a.mb_off[w] + idx - 1]), di));
+                        }
+                } else {
+                    if (idx >= setA.next) open_windows<0>(setA, a.mb_T, a.n_mb, idx);
+                    for (uint64_t m = setA.mask; m; m &= m - 1u) {
+                        const int w = __ffsll(static_cast<long long>(m)) - 1;
                         double &acc = mb_l2[w * T + tid];
                         acc = Rn::add(acc, Rn::div(Rn::mul(b_l1, a.mb_w[a.mb_off[w] + idx - 1]), di));
                     }
+                }
             }
             old_norm = new_norm;
         }
@@ -205,13 +279,20 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             if (a.n_ly) {
                 const double l = log(nv);
                 const uint64_t idx = a.ly_idx + k;
-                for (int w = 0; w < a.n_ly; ++w) {
+                if (!all_ly && idx >= setA.next) open_windows<1>(setA, a.ly_len, a.n_ly, idx);
+                uint64_t m = all_ly ? 0u : setA.mask;
+                for (int w = all_ly ? 0 : -1; all_ly ? w < a.n_ly : m != 0u;) {
+                    if (!all_ly) {
+                        w = __ffsll(static_cast<long long>(m)) - 1;
+                        m &= m - 1u;
+                    }
                     const uint64_t len = a.ly_len[w];
                     if (idx < len) {
                         ly_raw[w * T + tid] = Rn::add(ly_raw[w * T + tid], Rn::div(l, double(len)));
                         ly_b[w * T + tid] =
                             Rn::add(ly_b[w * T + tid], Rn::mul(l, a.ly_w[a.ly_off[w] + idx]));
                     }
+                    if (all_ly) ++w;
                 }
             }
 #pragma unroll
@@ -226,7 +307,13 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             store_x = ax;
             store_y = ay;
             const uint64_t idx = a.tu_idx + k;
-            for (int w = 0; w < a.n_tu; ++w) {
+            if (!all_tu && idx >= setB.next) open_windows<2>(setB, a.tu_T, a.n_tu, idx);
+            uint64_t m = all_tu ? 0u : setB.mask;
+            for (int w = all_tu ? 0 : -1; all_tu ? w < a.n_tu : m != 0u; w = all_tu ? w + 1 : w) {
+                if (!all_tu) {
+                    w = __ffsll(static_cast<long long>(m)) - 1;
+                    m &= m - 1u;
+                }
                 const uint64_t len = a.tu_T[w];
                 if (idx < len) {
                     const double wt = a.tu_w[a.tu_off[w] + idx];

@@ -182,14 +182,13 @@ namespace {
 struct PlanCache {
     std::mutex mutex;
     std::map<std::tuple<int, uint32_t, size_t>, cufftHandle> plans;
-    ~PlanCache() {
-        for (auto &kv : plans) cufftDestroy(kv.second);
-    }
 };
 
+// Never destroyed: at process exit the CUDA context may already be gone,
+// and the driver reclaims the plans' memory with it.
 PlanCache &plan_cache() {
-    static PlanCache c;
-    return c;
+    static PlanCache *c = new PlanCache;
+    return *c;
 }
 
 hm_status strided_plan(uint32_t len, size_t batch, cufftHandle *out) {

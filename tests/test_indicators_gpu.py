@@ -280,3 +280,29 @@ def test_storage_and_matrix_helpers(gpu):
     assert_bitwise(m.get(), np.tile(np.eye(4), (n, 1, 1)))
     with pytest.raises(ValueError, match="add_first"):
         C.TuneBirkhoff(n, [5]).add(p)
+
+
+def test_fused_many_windows_take_the_every_window_path(gpu):
+    # More than 64 windows of one kind (here 70 MEGNO-Birkhoff windows) are
+    # tested every turn instead of through the open-window bit set; both
+    # must give the per-call loop's values.
+    x, px, y, py = grid(0.5, 6)
+    n, n_turns = x.size, 300
+    mb_w = [int(t) for t in np.linspace(5, 400, 70).round()]
+    t = C.Tracker(n_turns + 1, TUNES[0], TUNES[1], "sps", NAN, 16.0, 0)
+    p = C.Particles(x, px, y, py)
+    M, Mo, mg, mb = C.Matrices(n), C.Matrices(n), C.Megno(n), C.MegnoBirkhoff(n, mb_w)
+    C.track_indicators(t, p, n_turns, 0.2, 10.0, matrix=M, matrix_old=Mo, megno=mg,
+                       megno_birkhoff=mb, megno_sample_turns=[7, 300], megno_samples_out=None)
+    t2 = C.Tracker(n_turns + 1, TUNES[0], TUNES[1], "sps", NAN, 16.0, 0)
+    p2 = C.Particles(x, px, y, py)
+    M2, Mo2, mg2, mb2 = C.Matrices(n), C.Matrices(n), C.Megno(n), C.MegnoBirkhoff(n, mb_w)
+    for _ in range(n_turns):
+        Mo2.explicit_copy(M2)
+        t2.track(p2, 1, 0.2, 10.0)
+        M2.structured_multiply(t2, p2, 0.2)
+        mg2.add(M2, Mo2)
+        mb2.add(M2, Mo2)
+    assert_bitwise(mb.get(), mb2.get(), "megno birkhoff, 70 windows")
+    assert_bitwise(mg.get(), mg2.get(), "megno")
+    assert_bitwise(M.get(), M2.get(), "matrices")
