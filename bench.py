@@ -259,7 +259,8 @@ def reference_cpu_sample(turns: int, side: int, repeats: int = 1, stride: int = 
 def bench_batched(C, arith, both_arith=True):
     """Mixed-size workload: 64 parameter sets, log-uniform 1k-256k particles
     in the 4D ball r < 0.6 and 1e3-1e6 turns, as one batch (graph replay)
-    versus one plain tracking call per set.  Survival counts must agree.
+    versus one plain tracking call per set at the tracker's tuned shape for
+    the same arithmetic.  Survival counts must agree.
     The batch runs the autotuner's shape for this GPU model and arithmetic
     (autotune.batch_shape: the committed cache, or a tuning run); with
     both_arith the other arithmetic is measured too, both arms in it."""
@@ -289,7 +290,10 @@ def bench_batched(C, arith, both_arith=True):
     b.run(True)
     t_one_group = time.perf_counter() - t0
     autotune.configure_batch(b, shape, arith)
-    # plain: one chunked tracking call per set on device arrays
+    # plain: one chunked tracking call per set on device arrays, at the
+    # tracker's own tuned shape for this arithmetic (restored afterwards)
+    saved_config, saved_staging = C.get_track_config(), C.get_track_staging()
+    plain_shape = autotune.apply(arith)
     t_plain, equal, o = 0.0, True, 0
     stream = torch.cuda.current_stream().cuda_stream
     for s in sets:
@@ -308,12 +312,15 @@ def bench_batched(C, arith, both_arith=True):
         t_plain += time.perf_counter() - t0
         equal &= bool(np.array_equal(st.cpu().numpy().view(np.uint32), steps_batch[o:o + n]))
         o += n
+    C.set_track_config(*saved_config)
+    C.set_track_staging(saved_staging)
     nominal = float(sum(s["n_particles"] * s["n_turns"] for s in sets))
     out = {"workload": "64 sets, tunes U[0.15,0.32], eps U[0,64], mu U[-0.5,0.5], "
                        "log-uniform 1e3-2.56e5 particles in the 4D ball r<0.6, "
                        "log-uniform 1e3-1e6 turns (seed 20261203)",
            "arith": "fast" if arith == C.ARITH_FAST else "exact",
            "tuned_shape": shape, "shape_source": "autotune.batch_shape (tuning.json)",
+           "plain_track_shape": plain_shape,
            "particles": int(sum(s["n_particles"] for s in sets)),
            "nominal_particle_turns": nominal, "executed_particle_turns": float(steps_batch.sum()),
            "batched_s": t_batch, "one_group_s": t_one_group, "plain_sum_s": t_plain,
@@ -323,8 +330,9 @@ def bench_batched(C, arith, both_arith=True):
     if both_arith:
         other = C.ARITH_FAST if arith == C.ARITH_EXACT else C.ARITH_EXACT
         o = bench_batched(C, other, both_arith=False)
-        out["other_arith"] = {k: o[k] for k in ("arith", "tuned_shape", "batched_s", "plain_sum_s",
-                                                  "speedup", "survival_equal_to_plain")}
+        out["other_arith"] = {k: o[k] for k in ("arith", "tuned_shape", "plain_track_shape",
+                                                  "batched_s", "plain_sum_s", "speedup",
+                                                  "survival_equal_to_plain")}
     return out
 
 
