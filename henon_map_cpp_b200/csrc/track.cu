@@ -15,6 +15,7 @@
 // henon_tracker_gpu::track, src/henon.cu:3155-3185.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "hm_device.cuh"
@@ -358,6 +359,21 @@ cudaError_t launch_s(const TrackChunk &c, unsigned blocks, int threads, cudaStre
     return cudaGetLastError();
 }
 
+// Multiprocessors of the current device (cached per device ordinal).
+int sm_count() {
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 1;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            return 1;
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
 template <int ARITH, bool OCT, bool REV>
 cudaError_t launch_k(const TrackChunk &c, const TrackLaunch &l, uint32_t n_upper,
                      cudaStream_t s) {
@@ -369,7 +385,15 @@ cudaError_t launch_k(const TrackChunk &c, const TrackLaunch &l, uint32_t n_upper
         if (blocks == 0) return cudaSuccess;
         return launch_s<ARITH, OCT, REV, 1, true>(c, blocks, threads, s);
     }
-    const int K = l.per_thread;
+    // Several particles per thread add instruction-level parallelism once
+    // the device is full; a short list would instead leave SMs idle (a
+    // particle is one serial chain of turns whatever its thread holds), so
+    // K is halved while the grid would give fewer than two blocks per SM.
+    int K = l.per_thread;
+    const uint64_t min_blocks = 2u * uint64_t(sm_count());
+    while (K > 1 && (uint64_t(n_upper) + uint64_t(threads) * K - 1) / (uint64_t(threads) * K) <
+                        min_blocks)
+        K /= 2;
     const uint64_t per_block = uint64_t(threads) * uint64_t(K);
     const unsigned blocks = unsigned((uint64_t(n_upper) + per_block - 1) / per_block);
     if (blocks == 0) return cudaSuccess;
