@@ -38,7 +38,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
 CU_SOURCES = ["track.cu", "noalloc.cu", "tangent.cu", "fused.cu", "ghosts.cu", "batch.cu",
               "adjoint.cu", "tunes.cu"]
 CPP_SOURCES = ["capi.cpp", "modulation.cpp", "indicators.cpp", "particles_extra.cpp",
-               "batch.cpp", "adjoint.cpp", "tunes.cpp"]
+               "batch.cpp", "adjoint.cpp", "tunes.cpp", "fft_plan.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

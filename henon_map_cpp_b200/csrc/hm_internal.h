@@ -371,7 +371,7 @@ struct OrbitRecordArgs {
     double mu;
     long long b2bits;
     int arith;
-    double *ox, *opx, *oy, *opy;  // orbit [n_turns + 1][n]
+    double *ox, *opx, *oy, *opy;  // orbit [n][n_turns + 1] (each particle's samples contiguous)
     // Optional (null when unused): each coordinate's sum over the samples,
     // from 0.0 in sample order ([4][n]), and the first sample holding NaN
     // (n_turns + 1 when none).
@@ -393,7 +393,7 @@ cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s);
 // segments in order.  Coordinates have means[c * n + i] subtracted first
 // when means is not null.
 struct BirkhoffSegArgs {
-    const double *x, *px, *y, *py;  // orbit [S][n]
+    const double *x, *px, *y, *py;  // orbit [n][S]
     const double *means;            // [4][n] or null
     const uint32_t *first_nan;      // [n]
     size_t n, S;
@@ -421,6 +421,51 @@ cudaError_t launch_fft_gather2(const double *x, const double *px, const double *
 cudaError_t launch_fft_peak2(const double2 *z, uint32_t len, size_t n, uint32_t last_sample,
                              const uint32_t *first_nan, double *out, size_t cols, int col,
                              cudaStream_t s);
+// FFT tunes of one window computed whole in one block's shared memory
+// (tunes.cu; plans in fft_plan.cpp): the DFT of the window's L samples is
+// an in-place mixed-radix network of length M (radices 2, 3, 4, 5, 8) when L
+// has no other prime factor (M = L), else Bluestein's chirp convolution
+// with M >= 2L - 1.  M is at most kFftMaxLen (the row fills at most 200 KB
+// of shared memory); longer windows take the library path above.
+constexpr int kFftMaxStages = 24;
+constexpr uint32_t kFftMaxLen = 12800;
+struct FftPlanDev {
+    uint32_t L = 0, M = 0;
+    int bluestein = 0;
+    int swizzle = 0;  // shared-memory slots XOR-swizzled (M a multiple of 8)
+    int n_stages = 0;
+    uint8_t radix[kFftMaxStages] = {};
+    uint32_t stage_len[kFftMaxStages] = {};   // span of the stage's butterflies
+    uint32_t stage_prod[kFftMaxStages] = {};  // product of the earlier radices
+    uint32_t n_coarse = 0;
+    const double2 *tw_coarse = nullptr;  // exp(-2 pi i 64 u / M), u < n_coarse
+    const double2 *tw_fine = nullptr;    // exp(-2 pi i v / M), v < 64
+    const uint32_t *pos = nullptr;       // direct: where X_k lies after the network
+    const double2 *chirp = nullptr;      // Bluestein: exp(-i pi n^2 / L), n < L
+    const double2 *bhat = nullptr;       // Bluestein: the network's output for b
+};
+// The plan of windows of L samples on the current device (built once, kept
+// until exit); *plan is null when L needs the library path.
+hm_status fft_plan(uint32_t L, const FftPlanDev **plan);
+// Shared-memory bytes of one block of fft_tune_kernel.
+size_t fft_tune_smem_bytes(const FftPlanDev &plan);
+
+struct FftTuneArgs {
+    const double *x, *px, *y, *py;  // orbit [n][S]
+    const double *means;            // [4][n] sums, or null
+    const uint32_t *first_nan;      // [n]
+    size_t n, S;
+    uint32_t from, last_sample;     // window samples from .. from + L - 1
+    const double *hann;             // [L]
+    double *out;                    // [n][cols]
+    size_t cols;
+    const int *out_cols;            // column pairs this window fills
+    int n_out_cols;
+    FftPlanDev plan;
+    uint32_t prefetch_ahead;        // set by launch_fft_tunes
+};
+cudaError_t launch_fft_tunes(const FftTuneArgs &a, cudaStream_t s);
+
 cudaError_t launch_mean_remove(double *x, double *px, double *y, double *py, size_t n, size_t S,
                                cudaStream_t s);
 cudaError_t launch_birkhoff_tunes(const double *x, const double *px, const double *y,

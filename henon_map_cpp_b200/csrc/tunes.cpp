@@ -175,13 +175,20 @@ hm_status hm_orbit_tunes_host(const double *x, const double *px, const double *y
 
 namespace {
 
-// cuFFT plans of the tracker's tune path, kept across calls: one per
-// (device, length, batch), rows of `length` contiguous values (fft_gather2
-// writes both planes' rows, batch = 2 particles).  Creating a plan costs
-// more than running it at these sizes.
+// cuFFT plans of the tracker's tune path (windows too long for the
+// shared-memory transform), kept across calls: one per (device, length,
+// batch), rows of `length` contiguous values (fft_gather2 writes both
+// planes' rows, batch = 2 particles).  Creating a plan costs more than
+// running it at these sizes.  Plans hold no work area of their own: each
+// call lends one from the library's pool (released with the call), so a
+// cached plan keeps no device memory between calls.
+struct CachedPlan {
+    cufftHandle plan = 0;
+    size_t work = 0;  // bytes of work area an execution needs
+};
 struct PlanCache {
     std::mutex mutex;
-    std::map<std::tuple<int, uint32_t, size_t>, cufftHandle> plans;
+    std::map<std::tuple<int, uint32_t, size_t>, CachedPlan> plans;
 };
 
 // Never destroyed: at process exit the CUDA context may already be gone,
@@ -191,7 +198,7 @@ PlanCache &plan_cache() {
     return *c;
 }
 
-hm_status strided_plan(uint32_t len, size_t batch, cufftHandle *out) {
+hm_status strided_plan(uint32_t len, size_t batch, CachedPlan *out) {
     int dev = 0;
     HM_CUDA_TRY(cudaGetDevice(&dev));
     PlanCache &c = plan_cache();
@@ -203,17 +210,52 @@ hm_status strided_plan(uint32_t len, size_t batch, cufftHandle *out) {
         return ok();
     }
     if (c.plans.size() >= 16) {  // bounded: drop the whole cache
-        for (auto &kv : c.plans) cufftDestroy(kv.second);
+        for (auto &kv : c.plans) cufftDestroy(kv.second.plan);
         c.plans.clear();
     }
-    cufftHandle plan = 0;
+    CachedPlan cp;
+    cufftResult r = cufftCreate(&cp.plan);
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "create");
     int nl = int(len);
-    const cufftResult r = cufftPlanMany(&plan, 1, &nl, nullptr, 1, nl, nullptr, 1, nl, CUFFT_Z2Z,
-                                        int(batch));
-    if (r != CUFFT_SUCCESS) return cufft_fail(r, "plan");
-    c.plans[key] = plan;
-    *out = plan;
+    r = cufftSetAutoAllocation(cp.plan, 0);
+    if (r == CUFFT_SUCCESS)
+        r = cufftMakePlanMany(cp.plan, 1, &nl, nullptr, 1, nl, nullptr, 1, nl, CUFFT_Z2Z,
+                              int(batch), &cp.work);
+    if (r != CUFFT_SUCCESS) {
+        cufftDestroy(cp.plan);
+        return cufft_fail(r, "plan");
+    }
+    c.plans[key] = cp;
+    *out = cp;
     return ok();
+}
+
+// Forward transform of `batch` rows of `len` values in place on the
+// default stream, with `work` (at least the plan's work area) lent to it.
+hm_status exec_strided(uint32_t len, size_t batch, double2 *z, DeviceBuffer &work) {
+    CachedPlan cp;
+    HM_TRY(strided_plan(len, batch, &cp));
+    HM_TRY(work.ensure(std::max<size_t>(cp.work, 1)));
+    PlanCache &c = plan_cache();
+    std::lock_guard<std::mutex> lock(c.mutex);  // stream and work area are per plan
+    HM_CUFFT_TRY_STREAM(cp.plan);
+    cufftResult r = cufftSetWorkArea(cp.plan, work.ptr);
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "work area");
+    auto *zc = reinterpret_cast<cufftDoubleComplex *>(z);
+    r = cufftExecZ2Z(cp.plan, zc, zc, CUFFT_FORWARD);
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "exec");
+    return ok();
+}
+
+// Work area per row of a library transform of `len` values (an estimate
+// over a batch of 1024 rows, doubled for margin).
+size_t fft_work_per_row(uint32_t len) {
+    size_t est = 0;
+    int nl = int(len);
+    if (cufftEstimateMany(1, &nl, nullptr, 1, nl, nullptr, 1, nl, CUFFT_Z2Z, 1024, &est) !=
+        CUFFT_SUCCESS)
+        return 8u * size_t(len) * sizeof(double2);
+    return 2u * (est / 1024u + 1u);
 }
 
 // One tune window of the tracker path: inclusive sample bounds, the NaN
@@ -297,36 +339,45 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
     HM_TRY(hm::upload(d_bcol, bcol));
     HM_TRY(hm::upload(d_boff, boff));
     HM_TRY(hm::upload(d_bw, bwts));
-    // Hann tables of the FFT windows.
-    uint32_t max_len = 0;
-    std::vector<DeviceBuffer> hann(fw.size());
+    // Hann tables of the FFT windows, and each window's transform: whole
+    // in shared memory when a plan exists for its length (fft_tune_kernel),
+    // else a library transform of rows gathered in global memory.
+    uint32_t max_len = 0;  // longest window of the library path
+    std::vector<DeviceBuffer> hann(fw.size()), fcols(fw.size());
+    std::vector<const hm::FftPlanDev *> fplan(fw.size(), nullptr);
     if (fft_out) {
         for (size_t j = 0; j < fw.size(); ++j) {
             const uint32_t L = fw[j].to - fw[j].from + 1;
-            max_len = std::max(max_len, L);
             HM_TRY(hann[j].alloc(size_t(L) * sizeof(double)));
             HM_CUDA_TRY(hm::launch_hann_table(hann[j].as<double>(), L, 0));
+            HM_TRY(hm::fft_plan(L, &fplan[j]));
+            if (fplan[j]) HM_TRY(hm::upload(fcols[j], fw[j].cols));
+            else max_len = std::max(max_len, L);
         }
     }
-    // Particle slice: the orbit (32 B per sample) plus the largest FFT
-    // window of both planes (32 B per sample) in at most two thirds of the
-    // free device memory.
+    // Particle slice: the orbit (32 B per sample) plus, for the library
+    // path's longest window, both planes' rows (32 B per sample) and the
+    // transform's work area, in at most two thirds of the free device
+    // memory.
     size_t free_b = 0;
     HM_TRY(hm::device_free_bytes(&free_b));
-    const size_t per_particle = S * 4 * sizeof(double) + size_t(max_len) * 2 * sizeof(double2);
+    const size_t per_particle = S * 4 * sizeof(double) +
+                                (max_len ? 2 * (size_t(max_len) * sizeof(double2) +
+                                                fft_work_per_row(max_len))
+                                         : 0u);
     const size_t slice = std::max<size_t>(1, std::min<size_t>(n, (free_b / 3 * 2) / per_particle));
     const size_t m0 = std::min(n, slice);
     // Segments of the Birkhoff sums: enough threads to fill the device.
     const uint32_t seg_len = std::max<uint32_t>(64u, uint32_t(std::min<size_t>(
                                                          S, (S * m0 * 2 + 262143) / 262144)));
     const uint32_t n_seg = uint32_t((S - 1 + seg_len - 1) / seg_len);
-    DeviceBuffer orbit, out, sums, first_nan, partial, z;
+    DeviceBuffer orbit, out, sums, first_nan, partial, z, fft_work;
     HM_TRY(orbit.alloc(m0 * S * 4 * sizeof(double)));
     HM_TRY(out.alloc(cols * m0 * sizeof(double)));
     if (remove_mean) HM_TRY(sums.alloc(4 * m0 * sizeof(double)));
     HM_TRY(first_nan.alloc(m0 * sizeof(uint32_t)));
     HM_TRY(partial.alloc(bf.size() * 2 * size_t(std::max<uint32_t>(n_seg, 1)) * m0 * sizeof(double)));
-    if (fft_out) HM_TRY(z.alloc(size_t(max_len) * 2 * m0 * sizeof(double2)));
+    if (fft_out && max_len) HM_TRY(z.alloc(size_t(max_len) * 2 * m0 * sizeof(double2)));
     const double b2 = barrier * barrier;
     long long b2bits = 0;
     if (!std::isnan(b2)) std::memcpy(&b2bits, &b2, sizeof(b2));
@@ -386,15 +437,31 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
         if (fft_out) {
             for (size_t j = 0; j < fw.size(); ++j) {
                 const uint32_t L = fw[j].to - fw[j].from + 1;
+                if (fplan[j]) {
+                    hm::FftTuneArgs f{};
+                    f.x = a.ox;
+                    f.px = a.opx;
+                    f.y = a.oy;
+                    f.py = a.opy;
+                    f.means = means;
+                    f.first_nan = a.first_nan;
+                    f.n = m;
+                    f.S = S;
+                    f.from = fw[j].from;
+                    f.last_sample = fw[j].to;
+                    f.hann = hann[j].as<double>();
+                    f.out = out.as<double>();
+                    f.cols = cols;
+                    f.out_cols = fcols[j].as<int>();
+                    f.n_out_cols = int(fw[j].cols.size());
+                    f.plan = *fplan[j];
+                    HM_CUDA_TRY(hm::launch_fft_tunes(f, 0));
+                    continue;
+                }
                 auto *zz = z.as<double2>();
                 HM_CUDA_TRY(hm::launch_fft_gather2(a.ox, a.opx, a.oy, a.opy, means, m, fw[j].from,
                                                    L, hann[j].as<double>(), zz, S, 0));
-                cufftHandle plan = 0;
-                HM_TRY(strided_plan(L, 2 * m, &plan));
-                HM_CUFFT_TRY_STREAM(plan);
-                auto *zc = reinterpret_cast<cufftDoubleComplex *>(zz);
-                const cufftResult r = cufftExecZ2Z(plan, zc, zc, CUFFT_FORWARD);
-                if (r != CUFFT_SUCCESS) return cufft_fail(r, "exec");
+                HM_TRY(exec_strided(L, 2 * m, zz, fft_work));
                 for (int c : fw[j].cols)
                     HM_CUDA_TRY(hm::launch_fft_peak2(zz, L, m, fw[j].to, a.first_nan,
                                                      out.as<double>(), cols, c, 0));

@@ -1,12 +1,8 @@
 // Tune estimates from turn-by-turn orbits (sm_100a).
 //
-// An orbit buffer holds S snapshots of n particles per coordinate, laid
-// out [sample][particle] (storage_4d_gpu's layout), so a warp reads 32
-// particles of one sample in one coalesced access.
-//
-// * orbit_record_kernel: tracks n_turns turns and writes every state
-//   (sample 0 = the start), like the reference's CPU tune routines that
-//   store the orbit before computing tunes (src/henon.cu:2890-3078);
+// Orbits the caller stored (storage tunes) hold S snapshots of n particles
+// per coordinate, laid out [sample][particle] (storage_4d_gpu's layout), so
+// a warp reads 32 particles of one sample in one coalesced access:
 // * mean_remove_kernel: subtracts each coordinate's orbit mean
 //   (src/henon.cu:3040-3051);
 // * birkhoff_kernel: Birkhoff-weighted phase advance over sample windows
@@ -15,15 +11,21 @@
 // * hann_gather_kernel + cuFFT + fft_peak_kernel: Hann-windowed spectrum of
 //   x + i px and the interpolated peak (compute_fft, interpolation, A,
 //   fft_tune_vec, src/dynamic_indicator.cpp:32-61, 134-196, 255-330).
-// Those serve orbits the caller stored (storage tunes).  The tracker's own
-// tune path records the orbit with each coordinate's running sum and the
-// first NaN sample, and then never rewrites it: the mean is subtracted as
-// samples are read, Birkhoff sums run in segments of turns over many
-// threads (birkhoff_seg_kernel / birkhoff_finish_kernel), and the FFT
-// gather writes both planes of a window as one batch of rows through
-// shared-memory tiles (fft_gather2_kernel, fft_peak2_kernel).
+// The tracker's own tune path (birkhoff_tunes / all_tunes,
+// src/henon.cu:2890-3078) records the orbit itself, particle-major
+// ([particle][sample] per coordinate: each particle's samples contiguous),
+// with each coordinate's running sum and the first NaN sample, and then
+// never rewrites it; the mean is subtracted as samples are read:
+// * orbit_record_kernel: tracks n_turns turns and writes every state
+//   (sample 0 = the start);
+// * birkhoff_seg_kernel / birkhoff_finish_kernel: Birkhoff sums in segments
+//   of turns over many threads;
+// * fft_tune_kernel: one window's spectrum computed whole in one block's
+//   shared memory, and its peak; windows too long for one block take
+//   fft_gather2_kernel + cuFFT + fft_peak2_kernel.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "hm_device.cuh"
@@ -41,27 +43,73 @@ using dev::Rn;
 // one).  Optionally each coordinate's sum over the samples (from 0.0, in
 // sample order: the reference's std::accumulate for all_tunes' mean,
 // src/henon.cu:3040-3051) and the first NaN sample.
+// The orbit is particle-major, so a warp's samples of one turn would land
+// in 32 different rows: each lane collects kRecGroup samples in shared
+// memory and the warp then writes them out as whole 128-byte lines (lanes
+// 0-15 one particle's run, lanes 16-31 the next).  Lanes past the last
+// particle run the loop on zeros (a fixed point) and write nothing.
+constexpr uint32_t kRecGroup = 16;
+
+__host__ __device__ constexpr size_t record_smem_bytes(int threads) {
+    return size_t(threads) * 4u * (kRecGroup + 1u) * sizeof(double);  // +1: bank padding
+}
+
 template <int ARITH, bool OCT, bool REV, bool KICK>
 __global__ void orbit_record_kernel(OrbitRecordArgs a) {
+    extern __shared__ double rec_stage[];  // [warp][coordinate][lane (kRecGroup + 1)]
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const size_t n = a.n;
-    double x = a.x[i], px = a.px[i], y = a.y[i], py = a.py[i];
-    uint32_t steps = a.steps[i];
-    bool alive = !dev::is_lost(x, px, y, py);
+    const bool valid = i < a.n;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const size_t n = a.n, S = size_t(a.n_turns) + 1u;
+    const size_t first_of_warp = i - lane;
+    constexpr uint32_t G = kRecGroup, W = G + 1u;
+    double *st = rec_stage + size_t(warp) * 4u * 32u * W;
+    double x = 0.0, px = 0.0, y = 0.0, py = 0.0;
+    uint32_t steps = 0;
+    if (valid) {
+        x = a.x[i];
+        px = a.px[i];
+        y = a.y[i];
+        py = a.py[i];
+        steps = a.steps[i];
+    }
+    bool alive = valid && !dev::is_lost(x, px, y, py);
     uint32_t first_nan = alive ? a.n_turns + 1u : 0u;
-    a.ox[i] = x;
-    a.opx[i] = px;
-    a.oy[i] = y;
-    a.opy[i] = py;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     const bool sums = a.sums != nullptr;
-    if (sums) {
-        s0 = Rn::add(s0, x);
-        s1 = Rn::add(s1, px);
-        s2 = Rn::add(s2, y);
-        s3 = Rn::add(s3, py);
-    }
+    // Sample s of this lane into the stage; the warp writes a full group
+    // (or the last, partial one) out.
+    auto put = [&](uint32_t s) {
+        const uint32_t g = s % G;
+        st[0 * 32u * W + lane * W + g] = x;
+        st[1 * 32u * W + lane * W + g] = px;
+        st[2 * 32u * W + lane * W + g] = y;
+        st[3 * 32u * W + lane * W + g] = py;
+        if (sums) {
+            s0 = Rn::add(s0, x);
+            s1 = Rn::add(s1, px);
+            s2 = Rn::add(s2, y);
+            s3 = Rn::add(s3, py);
+        }
+        if (g == G - 1u || s == a.n_turns) {
+            __syncwarp();
+            const uint32_t base = s - g, cnt = g + 1u;
+#pragma unroll
+            for (uint32_t v = lane; v < 32u * G; v += 32u) {
+                const uint32_t pl = v / G, gg = v % G;
+                const size_t ip = first_of_warp + pl;
+                if (gg < cnt && ip < n) {
+                    const size_t o = ip * S + base + gg;
+                    a.ox[o] = st[0 * 32u * W + pl * W + gg];
+                    a.opx[o] = st[1 * 32u * W + pl * W + gg];
+                    a.oy[o] = st[2 * 32u * W + pl * W + gg];
+                    a.opy[o] = st[3 * 32u * W + pl * W + gg];
+                }
+            }
+            __syncwarp();
+        }
+    };
+    put(0);
     dev::Particle p = dev::make_particle(x, px, y, py);
     const dev::Barrier bar = dev::make_barrier<ARITH>(a.b2bits);
     const unsigned long long id = a.id0 + i;
@@ -90,18 +138,9 @@ __global__ void orbit_record_kernel(OrbitRecordArgs a) {
                 first_nan = k + 1u;
             }
         }
-        const size_t o = size_t(k + 1) * n + i;
-        a.ox[o] = x;
-        a.opx[o] = px;
-        a.oy[o] = y;
-        a.opy[o] = py;
-        if (sums) {
-            s0 = Rn::add(s0, x);
-            s1 = Rn::add(s1, px);
-            s2 = Rn::add(s2, y);
-            s3 = Rn::add(s3, py);
-        }
+        put(k + 1u);
     }
+    if (!valid) return;
     a.x[i] = x;
     a.px[i] = px;
     a.y[i] = y;
@@ -171,10 +210,10 @@ __global__ void birkhoff_seg_kernel(const BirkhoffSegArgs a) {
             wb[j] = (long long)a.w_off[w0 + j] - (long long)lo[j];
         }
     }
-    double prev = atan2(centred(p[size_t(s0) * n + i], a.means, mp),
-                        centred(q[size_t(s0) * n + i], a.means, mq));
+    const size_t row = i * a.S;  // this particle's samples
+    double prev = atan2(centred(p[row + s0], a.means, mp), centred(q[row + s0], a.means, mq));
     for (uint32_t s = s0; s < s1; ++s) {
-        const size_t o = size_t(s + 1) * n + i;
+        const size_t o = row + s + 1u;
         const double th = atan2(centred(p[o], a.means, mp), centred(q[o], a.means, mq));
         double d = Rn::sub(th, prev);
         if (d < 0.0) d = Rn::add(d, 2.0 * M_PI);
@@ -218,47 +257,25 @@ __global__ void hann_table_kernel(double *h, uint32_t len) {
 
 // z[plane n + i][k] = ((q - mean) + i (p - mean)) h_k over the window's
 // samples from .. from + len - 1: one row of len values per column (plane,
-// particle), cuFFT's native batch layout.  A block moves a tile of 32
-// samples x 32 columns through shared memory, so that the orbit is read
-// along particles and the rows are written along samples, both coalesced.
-constexpr int kTile = 32;
-
+// particle), cuFFT's native batch layout.  The orbit's samples are
+// contiguous per particle, so rows are read and written along samples.
 __global__ void __launch_bounds__(256) fft_gather2_kernel(const double *x, const double *px,
                                                           const double *y, const double *py,
                                                           const double *means, size_t n,
                                                           uint32_t from, uint32_t len,
                                                           const double *h, double2 *z, size_t S,
                                                           int plane) {
-    __shared__ double2 tile[kTile][kTile + 1];
-    const size_t i0 = size_t(blockIdx.x) * kTile;  // first particle of the tile
-    const uint32_t k0 = blockIdx.y * kTile;        // first sample of the tile
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n * len) return;
+    const size_t i = t / len;
+    const uint32_t k = uint32_t(t - i * len);
     const double *q = plane ? y : x, *p = plane ? py : px;
-    const unsigned tx = threadIdx.x & 31u, ty = threadIdx.x >> 5;  // 8 warps
-    // read: lane tx takes particle i0 + tx; warp ty samples k0 + ty, + 8, ...
-    {
-        const size_t i = i0 + tx;
-        const bool ok_i = i < n;
-        const double mq = ok_i ? mean_of(means, n, i, 2 * plane, S) : 0.0;
-        const double mp = ok_i ? mean_of(means, n, i, 2 * plane + 1, S) : 0.0;
-        for (unsigned r = ty; r < unsigned(kTile); r += 8u) {
-            const uint32_t k = k0 + r;
-            double2 v = make_double2(0.0, 0.0);
-            if (ok_i && k < len) {
-                const size_t o = size_t(from + k) * n + i;
-                const double re = centred(q[o], means, mq), im = centred(p[o], means, mp);
-                const double hk = h[k];
-                v = make_double2(re * hk, im * hk);
-            }
-            tile[r][tx] = v;
-        }
-    }
-    __syncthreads();
-    // write: warp ty takes particles i0 + ty, + 8, ...; lane tx sample k0 + tx
-    for (unsigned ii = ty; ii < unsigned(kTile); ii += 8u) {
-        const size_t i = i0 + ii;
-        const uint32_t k = k0 + tx;
-        if (i < n && k < len) z[(size_t(plane) * n + i) * len + k] = tile[tx][ii];
-    }
+    const double mq = mean_of(means, n, i, 2 * plane, S);
+    const double mp = mean_of(means, n, i, 2 * plane + 1, S);
+    const size_t o = i * S + from + k;
+    const double re = centred(q[o], means, mq), im = centred(p[o], means, mp);
+    const double hk = h[k];
+    z[(size_t(plane) * n + i) * len + k] = make_double2(re * hk, im * hk);
 }
 
 // One warp per column (plane, particle): first maximum of |z_k| over k
@@ -488,15 +505,375 @@ __global__ void fft_peak_kernel(const double2 *buf, uint32_t len, size_t count,
     out[(first + warp) * out_stride] = value;
 }
 
+// ---- FFT tunes in shared memory --------------------------------------------------
+// One block per row (plane, particle) of one window: the samples are read
+// from the orbit (mean subtracted, Hann window applied) into shared memory,
+// transformed there, and the block writes the interpolated peak.  The
+// transform of length M is an in-place mixed-radix network of radices 2, 3,
+// 4, 5 and 8.  Forward, decimation in frequency: stage s splits each block of
+// N = r * span values (radix r) into r butterflies of stride `span`,
+//     y_k = sum_q x_q w_r^{qk},  stored times w_N^{jk} (j: offset in the span),
+// which takes natural order in and leaves X_k at a digit-reversed position
+// (FftPlanDev::pos).  The inverse network runs the stages backwards with
+// conjugate twiddles applied before each butterfly (decimation in time),
+// which takes that order back to natural order (times M).  Bluestein's
+// convolution (L. Bluestein, "A linear filtering approach to the
+// computation of the discrete Fourier transform", IEEE Trans. Audio
+// Electroacoust. 18 (1970) 451-455) uses both:
+//     X_k = c_k sum_n (z_n c_n) conj(c_{k-n}),  c_n = exp(-i pi n^2 / L),
+// the cyclic convolution of length M >= 2L - 1 being the inverse network of
+// the pointwise product of the forward network's outputs (that of b_m =
+// conj(c_m) is precomputed, in the same order).  |c_k| = 1 and the peak
+// interpolation depends on magnitude ratios only, so the peak is taken on
+// |conv_k| directly.
+
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) {
+    return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {  // a b
+    return make_double2(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 c_mulc(double2 a, double2 b) {  // a conj(b)
+    return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -(a.x * b.y)));
+}
+__device__ __forceinline__ double2 c_i(double2 a) {  // i a
+    return make_double2(-a.y, a.x);
+}
+
+// Shared-memory slots of a row: M rounded up to a multiple of 8.
+__host__ __device__ __forceinline__ uint32_t fft_row_slots(const FftPlanDev &pl) {
+    return (pl.M + 7u) & ~7u;
+}
+
+// exp(-2 pi i t / M) from the two shared-memory tables (t < M).
+__device__ __forceinline__ double2 fft_twiddle(const double2 *coarse, const double2 *fine,
+                                               uint32_t t) {
+    return c_mul(coarse[t >> 6], fine[t & 63u]);
+}
+
+// The DFT of R values in registers (R = 2, 3, 4, 5, 8), forward
+// (w = exp(-2 pi i / R)) or inverse (conjugate w).
+template <bool INV>
+__device__ __forceinline__ void dft4(double2 &x0, double2 &x1, double2 &x2, double2 &x3) {
+    const double2 t0 = c_add(x0, x2), t1 = c_sub(x0, x2);
+    const double2 t2 = c_add(x1, x3), t3 = c_sub(x1, x3);
+    const double2 it3 = c_i(t3);
+    x0 = c_add(t0, t2);
+    x2 = c_sub(t0, t2);
+    x1 = INV ? c_add(t1, it3) : c_sub(t1, it3);
+    x3 = INV ? c_sub(t1, it3) : c_add(t1, it3);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft_small(double2 (&v)[R]) {
+    if constexpr (R == 2) {
+        const double2 a = v[0], b = v[1];
+        v[0] = c_add(a, b);
+        v[1] = c_sub(a, b);
+    } else if constexpr (R == 4) {
+        dft4<INV>(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 8) {
+        // even and odd halves, then X_k = E_k + w8^k O_k, X_{k+4} = E_k - w8^k O_k
+        double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+        double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+        dft4<INV>(e0, e1, e2, e3);
+        dft4<INV>(o0, o1, o2, o3);
+        constexpr double h = 0.70710678118654752440;  // sqrt(2) / 2
+        // w8 o1, w8^2 o2, w8^3 o3 (forward w8 = h (1 - i); inverse h (1 + i))
+        const double2 p1 = INV ? make_double2(h * (o1.x - o1.y), h * (o1.x + o1.y))
+                               : make_double2(h * (o1.x + o1.y), h * (o1.y - o1.x));
+        const double2 p2 = INV ? c_i(o2) : make_double2(o2.y, -o2.x);
+        const double2 p3 = INV ? make_double2(-h * (o3.x + o3.y), h * (o3.x - o3.y))
+                               : make_double2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+        v[0] = c_add(e0, o0);
+        v[4] = c_sub(e0, o0);
+        v[1] = c_add(e1, p1);
+        v[5] = c_sub(e1, p1);
+        v[2] = c_add(e2, p2);
+        v[6] = c_sub(e2, p2);
+        v[3] = c_add(e3, p3);
+        v[7] = c_sub(e3, p3);
+    } else if constexpr (R == 5) {
+        // cos(2 pi / 5), cos(4 pi / 5), sin(2 pi / 5), sin(4 pi / 5)
+        constexpr double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+        constexpr double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+        const double2 x0 = v[0];
+        const double2 t1 = c_add(v[1], v[4]), t2 = c_add(v[2], v[3]);
+        const double2 u1 = c_sub(v[1], v[4]), u2 = c_sub(v[2], v[3]);
+        v[0] = c_add(x0, c_add(t1, t2));
+        const double2 a1 = make_double2(fma(c2, t2.x, fma(c1, t1.x, x0.x)),
+                                        fma(c2, t2.y, fma(c1, t1.y, x0.y)));
+        const double2 a2 = make_double2(fma(c1, t2.x, fma(c2, t1.x, x0.x)),
+                                        fma(c1, t2.y, fma(c2, t1.y, x0.y)));
+        const double2 ib1 = c_i(make_double2(fma(s1, u1.x, s2 * u2.x), fma(s1, u1.y, s2 * u2.y)));
+        const double2 ib2 = c_i(make_double2(fma(s2, u1.x, -(s1 * u2.x)),
+                                             fma(s2, u1.y, -(s1 * u2.y))));
+        v[1] = INV ? c_add(a1, ib1) : c_sub(a1, ib1);
+        v[4] = INV ? c_sub(a1, ib1) : c_add(a1, ib1);
+        v[2] = INV ? c_add(a2, ib2) : c_sub(a2, ib2);
+        v[3] = INV ? c_sub(a2, ib2) : c_add(a2, ib2);
+    } else {
+        static_assert(R == 3, "radix");
+        constexpr double s = 0.86602540378443864676;  // sin(2 pi / 3)
+        const double2 x0 = v[0];
+        const double2 t = c_add(v[1], v[2]), u = c_sub(v[1], v[2]);
+        v[0] = c_add(x0, t);
+        const double2 a = make_double2(fma(-0.5, t.x, x0.x), fma(-0.5, t.y, x0.y));
+        const double2 ib = c_i(make_double2(s * u.x, s * u.y));
+        v[1] = INV ? c_add(a, ib) : c_sub(a, ib);
+        v[2] = INV ? c_sub(a, ib) : c_add(a, ib);
+    }
+}
+
+// Shared-memory slot of row value i: with SWZ the low three bits of i (its
+// place among 8 consecutive values, one 128-byte bank row of double2) are
+// XORed with the next three, so that the small strides of the last stages
+// (radices 8, 4, 2 run last) fall into different banks.  A bijection on
+// every aligned group of 8, so rows of a multiple of 8 values stay in place.
+template <bool SWZ>
+__device__ __forceinline__ uint32_t slot(uint32_t i) {
+    return SWZ ? (i ^ ((i >> 3) & 7u)) : i;
+}
+
+// w^k for k < 8 from w, w^2 and w^4 (at most two products deep).
+__device__ __forceinline__ double2 twiddle_pow(int k, double2 w1, double2 w2, double2 w4) {
+    switch (k) {
+        case 1: return w1;
+        case 2: return w2;
+        case 3: return c_mul(w1, w2);
+        case 4: return w4;
+        case 5: return c_mul(w1, w4);
+        case 6: return c_mul(w2, w4);
+        default: return c_mul(c_mul(w1, w2), w4);
+    }
+}
+
+// One stage of radix R over row[0, M): butterfly b (b < M / R) covers
+// block b / span at offset j = b % span; the twiddles w_N^{jk}, N = R span,
+// are exp(-2 pi i j k prod / M) = w^k with w from the tables.  Forward:
+// butterfly, then twiddles; inverse: conjugate twiddles, then the inverse
+// butterfly.  A stage of span 1 has j = 0 and no twiddles (TW false).
+template <int R, bool INV, bool SWZ, bool TW>
+__device__ __forceinline__ void fft_stage(double2 *row, uint32_t M, uint32_t span, uint32_t prod,
+                                          const double2 *tc, const double2 *tf) {
+    const uint32_t nb = M / R, T = blockDim.x;
+    uint32_t blk = threadIdx.x / span, j = threadIdx.x - blk * span;
+    const uint32_t dq = T / span, dr = T - dq * span;
+    constexpr int kUnroll = R >= 8 ? 1 : 2;  // radix 8 fills the registers alone
+#pragma unroll kUnroll
+    for (uint32_t b = threadIdx.x; b < nb; b += T) {
+        const uint32_t base = blk * span * R + j;
+        double2 w1 = make_double2(1.0, 0.0), w2 = w1, w4 = w1;
+        if (TW) {
+            w1 = fft_twiddle(tc, tf, j * prod);
+            w2 = c_mul(w1, w1);
+            w4 = c_mul(w2, w2);
+        }
+        double2 v[R];
+        if (!INV) {
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[q] = row[slot<SWZ>(base + q * span)];
+            dft_small<R, false>(v);
+#pragma unroll
+            for (int k = 0; k < R; ++k)
+                row[slot<SWZ>(base + k * span)] =
+                    (TW && k > 0) ? c_mul(v[k], twiddle_pow(k, w1, w2, w4)) : v[k];
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                const double2 x = row[slot<SWZ>(base + q * span)];
+                v[q] = (TW && q > 0) ? c_mulc(x, twiddle_pow(q, w1, w2, w4)) : x;
+            }
+            dft_small<R, true>(v);
+#pragma unroll
+            for (int k = 0; k < R; ++k) row[slot<SWZ>(base + k * span)] = v[k];
+        }
+        blk += dq;
+        j += dr;
+        if (j >= span) {
+            j -= span;
+            ++blk;
+        }
+    }
+}
+
+template <int R, bool INV, bool SWZ>
+__device__ __forceinline__ void fft_stage_any(double2 *row, uint32_t M, uint32_t span,
+                                              uint32_t prod, const double2 *tc,
+                                              const double2 *tf) {
+    if (span == 1) fft_stage<R, INV, SWZ, false>(row, M, span, prod, tc, tf);
+    else fft_stage<R, INV, SWZ, true>(row, M, span, prod, tc, tf);
+}
+
+// The forward (decimation in frequency) or inverse (decimation in time)
+// network in place over the row; the caller synchronises before.
+template <bool INV, bool SWZ>
+__device__ void fft_network(double2 *row, const FftPlanDev &pl, const double2 *tc,
+                            const double2 *tf) {
+    for (int t = 0; t < pl.n_stages; ++t) {
+        const int s = INV ? pl.n_stages - 1 - t : t;
+        const uint32_t span = pl.stage_len[s], prod = pl.stage_prod[s];
+        switch (pl.radix[s]) {
+            case 8: fft_stage_any<8, INV, SWZ>(row, pl.M, span, prod, tc, tf); break;
+            case 4: fft_stage_any<4, INV, SWZ>(row, pl.M, span, prod, tc, tf); break;
+            case 2: fft_stage_any<2, INV, SWZ>(row, pl.M, span, prod, tc, tf); break;
+            case 5: fft_stage_any<5, INV, SWZ>(row, pl.M, span, prod, tc, tf); break;
+            default: fft_stage_any<3, INV, SWZ>(row, pl.M, span, prod, tc, tf); break;
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int kFftThreadsMax = 1024;
+
+template <bool SWZ>
+__global__ void __launch_bounds__(kFftThreadsMax) fft_tune_kernel(const FftTuneArgs a) {
+    extern __shared__ __align__(16) double2 fft_sm[];
+    __shared__ double red_m[kFftThreadsMax / 32];
+    __shared__ uint32_t red_k[kFftThreadsMax / 32];
+    const FftPlanDev &pl = a.plan;
+    double2 *row = fft_sm;
+    double2 *tc = row + fft_row_slots(pl);
+    double2 *tf = tc + pl.n_coarse;
+    const size_t rix = blockIdx.x;  // plane * n + particle
+    const int plane = rix >= a.n ? 1 : 0;
+    const size_t i = rix - size_t(plane) * a.n;
+    // Only one or a few rows fit in an SM's shared memory, so a block's
+    // reads would not overlap other rows' transforms: each block asks L2 for
+    // the window of the row that starts about one wave of resident blocks
+    // later (prefetch.global.L2, one per 128-byte line, addresses within
+    // the row).
+    {
+        const size_t r2 = rix + a.prefetch_ahead;
+        if (r2 < 2 * a.n) {
+            const int plane2 = r2 >= a.n ? 1 : 0;
+            const size_t i2 = r2 - size_t(plane2) * a.n;
+            const size_t bytes = size_t(pl.L) * sizeof(double);
+            const char *rq = reinterpret_cast<const char *>((plane2 ? a.y : a.x) + i2 * a.S + a.from);
+            const char *rp = reinterpret_cast<const char *>((plane2 ? a.py : a.px) + i2 * a.S + a.from);
+            const uint32_t lines = uint32_t((bytes + 127u) / 128u) + 1u;
+            for (uint32_t l = threadIdx.x; l < 2u * lines; l += blockDim.x) {
+                const size_t off = min(size_t(l % lines) * 128u, bytes - sizeof(double));
+                const char *ptr = (l < lines ? rq : rp) + off;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+            }
+        }
+    }
+    if (a.first_nan[i] <= a.last_sample) {  // a NaN sample in the window: NaN tune
+        if (threadIdx.x == 0)
+            for (int c = 0; c < a.n_out_cols; ++c)
+                a.out[i * a.cols + 2 * size_t(a.out_cols[c]) + plane] = dev::quiet_nan();
+        return;
+    }
+    for (uint32_t t = threadIdx.x; t < pl.n_coarse; t += blockDim.x) tc[t] = pl.tw_coarse[t];
+    for (uint32_t t = threadIdx.x; t < 64u; t += blockDim.x) tf[t] = pl.tw_fine[t];
+    const double *q = plane ? a.y : a.x, *p = plane ? a.py : a.px;
+    const double mq = mean_of(a.means, a.n, i, 2 * plane, a.S);
+    const double mp = mean_of(a.means, a.n, i, 2 * plane + 1, a.S);
+    // z_k = ((q - mean) + i (p - mean)) h_k.  Bluestein: z_k c_k in natural
+    // order (zeros up to M) for the forward network.  Direct: conj(z_k) at
+    // the forward network's position of k, so that the inverse network
+    // gives conj(X_k) in natural order (the magnitudes are those of X_k).
+#pragma unroll 4
+    for (uint32_t k = threadIdx.x; k < pl.M; k += blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        if (k < pl.L) {
+            const size_t o = i * a.S + a.from + k;
+            const double re = centred(q[o], a.means, mq), im = centred(p[o], a.means, mp);
+            const double hk = a.hann[k];
+            v = make_double2(re * hk, im * hk);
+            if (pl.bluestein) v = c_mul(v, pl.chirp[k]);
+            else v.y = -v.y;
+        }
+        row[slot<SWZ>(pl.bluestein ? k : pl.pos[k])] = v;
+    }
+    __syncthreads();
+    if (pl.bluestein) {
+        fft_network<false, SWZ>(row, pl, tc, tf);
+        for (uint32_t k = threadIdx.x; k < pl.M; k += blockDim.x)
+            row[slot<SWZ>(k)] = c_mul(row[slot<SWZ>(k)], pl.bhat[k]);
+        __syncthreads();
+    }
+    fft_network<true, SWZ>(row, pl, tc, tf);
+    auto at = [&](uint32_t k) { return row[slot<SWZ>(k)]; };
+    // First maximum of |X_k| (squared, monotone) over k < L; k grows within
+    // a thread, and ties across threads keep the smallest k.
+    double best = -1.0;
+    uint32_t best_k = 0xffffffffu;
+    for (uint32_t k = threadIdx.x; k < pl.L; k += blockDim.x) {
+        const double2 v = at(k);
+        const double m2 = v.x * v.x + v.y * v.y;
+        if (m2 > best) {
+            best = m2;
+            best_k = k;
+        }
+    }
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(dev::kFullMask, best, o);
+        const uint32_t ok = __shfl_down_sync(dev::kFullMask, best_k, o);
+        if (ob > best || (ob == best && ok < best_k)) {
+            best = ob;
+            best_k = ok;
+        }
+    }
+    if (lane == 0) {
+        red_m[warp] = best;
+        red_k[warp] = best_k;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (unsigned w = 1; w < blockDim.x / 32u; ++w)
+        if (red_m[w] > best || (red_m[w] == best && red_k[w] < best_k)) {
+            best = red_m[w];
+            best_k = red_k[w];
+        }
+    auto mag = [&](uint32_t k) {
+        const double2 v = at(k);
+        return sqrt(v.x * v.x + v.y * v.y);
+    };
+    // interpolation (src/dynamic_indicator.cpp:139-176), as fft_peak2_kernel
+    const uint32_t len = pl.L;
+    double value;
+    uint32_t index = best_k;
+    const double N = double(len);
+    if (index == 0 || index >= len) {
+        value = 1.0;
+    } else if (index == len - 1) {
+        value = 0.0;
+    } else {
+        uint32_t i1, i2;
+        if (mag(index - 1) > mag(index + 1)) {
+            i1 = index - 1;
+            i2 = index;
+            index = index - 1;
+        } else {
+            i1 = index;
+            i2 = index + 1;
+        }
+        const double v = (double(index) / N) +
+                         (1.0 / (2.0 * M_PI)) *
+                             asin(interp_a(mag(i1), mag(i2), cos(2.0 * M_PI / N)) *
+                                  sin(2.0 * M_PI / N));
+        value = fabs(1.0 - v);
+    }
+    for (int c = 0; c < a.n_out_cols; ++c)
+        a.out[i * a.cols + 2 * size_t(a.out_cols[c]) + plane] = value;
+}
+
 template <int ARITH, bool OCT>
 void launch_record_ok(const OrbitRecordArgs &a, unsigned blocks, int threads, cudaStream_t s) {
     const bool kick = !isnan(a.kick_module);
+    const size_t smem = record_smem_bytes(threads);
     if (a.inverse) {
-        if (kick) orbit_record_kernel<ARITH, OCT, true, true><<<blocks, threads, 0, s>>>(a);
-        else orbit_record_kernel<ARITH, OCT, true, false><<<blocks, threads, 0, s>>>(a);
+        if (kick) orbit_record_kernel<ARITH, OCT, true, true><<<blocks, threads, smem, s>>>(a);
+        else orbit_record_kernel<ARITH, OCT, true, false><<<blocks, threads, smem, s>>>(a);
     } else {
-        if (kick) orbit_record_kernel<ARITH, OCT, false, true><<<blocks, threads, 0, s>>>(a);
-        else orbit_record_kernel<ARITH, OCT, false, false><<<blocks, threads, 0, s>>>(a);
+        if (kick) orbit_record_kernel<ARITH, OCT, false, true><<<blocks, threads, smem, s>>>(a);
+        else orbit_record_kernel<ARITH, OCT, false, false><<<blocks, threads, smem, s>>>(a);
     }
 }
 
@@ -504,9 +881,10 @@ void launch_record_ok(const OrbitRecordArgs &a, unsigned blocks, int threads, cu
 
 cudaError_t launch_orbit_record(const OrbitRecordArgs &a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
-    // Small blocks: the orbit of few particles is a long serial chain, so
-    // spread the threads over as many SMs as possible.
-    const int threads = a.n < 148u * 128u ? 32 : 128;
+    // One warp per block: the orbit of few particles is a long serial chain,
+    // spread over as many SMs as possible, and the staging buffer (17 KB a
+    // warp) sets the residency, not the block size.
+    const int threads = 32;
     const unsigned blocks = unsigned((a.n + threads - 1) / threads);
     const bool oct = a.mu != 0.0;
     if (a.arith == HM_ARITH_FAST) {
@@ -542,7 +920,7 @@ cudaError_t launch_fft_gather2(const double *x, const double *px, const double *
                                uint32_t len, const double *h, double2 *z, size_t S,
                                cudaStream_t s) {
     if (n == 0 || len == 0) return cudaSuccess;
-    const dim3 grid(unsigned((n + kTile - 1) / kTile), (len + kTile - 1) / kTile);
+    const unsigned grid = unsigned((n * len + 255) / 256);
     for (int plane = 0; plane < 2; ++plane) {
         fft_gather2_kernel<<<grid, 256, 0, s>>>(x, px, y, py, means, n, from, len, h, z, S, plane);
         const cudaError_t e = cudaGetLastError();
@@ -558,6 +936,39 @@ cudaError_t launch_fft_peak2(const double2 *z, uint32_t len, size_t n, uint32_t 
     const size_t threads = 2 * n * 32;
     fft_peak2_kernel<<<unsigned((threads + 255) / 256), 256, 0, s>>>(z, len, n, last_sample,
                                                                     first_nan, out, cols, col);
+    return cudaGetLastError();
+}
+
+size_t fft_tune_smem_bytes(const FftPlanDev &plan) {
+    return (size_t(fft_row_slots(plan)) + plan.n_coarse + 64u) * sizeof(double2);
+}
+
+cudaError_t launch_fft_tunes(const FftTuneArgs &a, cudaStream_t s) {
+    if (a.n == 0) return cudaSuccess;
+    if (a.plan.M == 0 || a.plan.M > kFftMaxLen || a.plan.L == 0) return cudaErrorInvalidValue;
+    const size_t smem = fft_tune_smem_bytes(a.plan);
+    auto kernel = a.plan.swizzle ? fft_tune_kernel<true> : fft_tune_kernel<false>;
+    if (smem > 40u * 1024u) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    // About one radix-8 butterfly per thread and stage.  A row of 6144
+    // values or more fills most of an SM's shared memory, so its block takes
+    // up to 1024 threads; shorter rows take 256, so that several blocks share
+    // an SM.
+    const uint32_t want = (a.plan.M / 8u + 31u) / 32u * 32u;
+    const uint32_t cap = a.plan.M >= 6144u ? uint32_t(kFftThreadsMax) : 256u;
+    const int threads = int(std::min<uint32_t>(cap, std::max<uint32_t>(64u, want)));
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (e != cudaSuccess) return e;
+    FftTuneArgs b = a;
+    b.prefetch_ahead = uint32_t(std::max(1, sms * std::max(1, per_sm)));
+    kernel<<<unsigned(2 * a.n), threads, smem, s>>>(b);
     return cudaGetLastError();
 }
 

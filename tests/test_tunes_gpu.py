@@ -64,6 +64,31 @@ def test_tracker_orbit_tunes_match_oracle(gpu, remove_mean):
     np.testing.assert_array_equal(steps, want[4])
 
 
+@pytest.mark.parametrize("remove_mean", [False, True])
+def test_tracker_fft_tunes_window_lengths(gpu, remove_mean):
+    # Window lengths across the transform's cases: one sample; lengths of
+    # radices 2, 3, 4 and 5 only, transformed directly (up to the longest
+    # row one block holds, 12800); Bluestein's convolution for other
+    # lengths (7, 1001 = 7 * 11 * 13, the prime 4001, 5001 = 3 * 1667, and
+    # 6400, whose convolution of 12799 values takes the longest row); and
+    # lengths beyond both (6401, 12801), which take the library transform.
+    x, px, y, py = grid(0.25, 3, px0=0.001)
+    lengths = [1, 2, 3, 7, 16, 64, 125, 1001, 4001, 5001, 6400, 6401, 10000, 12800, 12801]
+    n_turns = 13000
+    frm = [(37 * j) % 150 for j in range(len(lengths))]
+    to = [f + n - 1 for f, n in zip(frm, lengths)]
+    tr = C.Tracker(n_turns, *TUNES, "sps", NAN, 8.0, 0)
+    p = C.Particles(x, px, y, py)
+    _, f = C.tracker_orbit_tunes(tr, p, n_turns, 0.0, 10.0, frm, to, remove_mean, True)
+    orb = T.orbit(x, px, y, py, O.tables(n_turns, *TUNES, "sps", epsilon=8.0), n_turns, 0.0)
+    if remove_mean:
+        orb = T.remove_mean(orb)
+    want = np.array([T.tune_vec(*(orb[c, :, i] for c in range(4)), frm, to, "fft")
+                     for i in range(x.size)])
+    assert np.isfinite(want).all()
+    _close(f, want, 1e-10, "fft")
+
+
 def test_storage_tunes_match_oracle(gpu):
     x, px, y, py = grid(0.3, 6)
     n = x.size
