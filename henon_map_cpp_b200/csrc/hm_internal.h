@@ -451,10 +451,13 @@ hm_status fft_plan(uint32_t L, const FftPlanDev **plan);
 size_t fft_tune_smem_bytes(const FftPlanDev &plan);
 
 struct FftTuneArgs {
-    const double *x, *px, *y, *py;  // orbit [n][S]
+    const double *x, *px, *y, *py;  // orbit: sample s of particle i at i stride_i + s stride_s
     const double *means;            // [4][n] sums, or null
-    const uint32_t *first_nan;      // [n]
+    // [n] first NaN sample of each particle; null: the block scans its
+    // window instead (NaN tune when any of its samples is NaN)
+    const uint32_t *first_nan;
     size_t n, S;
+    size_t stride_i, stride_s;      // (S, 1): the tracker's orbit; (1, n): stored orbits
     uint32_t from, last_sample;     // window samples from .. from + L - 1
     const double *hann;             // [L]
     double *out;                    // [n][cols]

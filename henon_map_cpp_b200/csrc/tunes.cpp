@@ -61,8 +61,9 @@ hm_status birkhoff_device(const double *x, const double *px, const double *y, co
     return ok();
 }
 
-// FFT tunes of the windows (from, to) plus the full orbit [1, S-1], in
-// particle slices bounded by the spectrum buffer.
+// FFT tunes of the windows (from, to) plus the full orbit [1, S-1]: in
+// shared memory (fft_tune_kernel) where the window fits one block, else in
+// particle slices bounded by the spectrum buffer through cuFFT.
 hm_status fft_device(const double *x, const double *px, const double *y, const double *py,
                      size_t n, size_t S, const std::vector<uint32_t> &from,
                      const std::vector<uint32_t> &to, double *dev_out) {
@@ -75,6 +76,35 @@ hm_status fft_device(const double *x, const double *px, const double *y, const d
     for (size_t j = 0; j < f.size(); ++j) {
         const uint32_t L = len[j];
         if (L == 0) continue;
+        // Windows one block holds: transformed in shared memory, every
+        // particle in one launch, the window's own samples deciding NaN.
+        const hm::FftPlanDev *plan = nullptr;
+        HM_TRY(hm::fft_plan(L, &plan));
+        if (plan) {
+            DeviceBuffer hann, col;
+            HM_TRY(hann.alloc(size_t(L) * sizeof(double)));
+            HM_CUDA_TRY(hm::launch_hann_table(hann.as<double>(), L, 0));
+            HM_TRY(hm::upload(col, std::vector<int>{int(j)}));
+            hm::FftTuneArgs a{};
+            a.x = x;
+            a.px = px;
+            a.y = y;
+            a.py = py;
+            a.n = n;
+            a.S = S;
+            a.stride_i = 1;
+            a.stride_s = n;
+            a.from = f[j];
+            a.last_sample = f[j] + L - 1;
+            a.hann = hann.as<double>();
+            a.out = dev_out;
+            a.cols = cols;
+            a.out_cols = col.as<int>();
+            a.n_out_cols = 1;
+            a.plan = *plan;
+            HM_CUDA_TRY(hm::launch_fft_tunes(a, 0));
+            continue;
+        }
         const size_t slice = std::max<size_t>(1, std::min(n, budget / (size_t(L) * sizeof(double2))));
         DeviceBuffer buf, flags;
         HM_TRY(buf.alloc(slice * L * sizeof(double2)));
@@ -447,6 +477,8 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
                     f.first_nan = a.first_nan;
                     f.n = m;
                     f.S = S;
+                    f.stride_i = S;
+                    f.stride_s = 1;
                     f.from = fw[j].from;
                     f.last_sample = fw[j].to;
                     f.hann = hann[j].as<double>();

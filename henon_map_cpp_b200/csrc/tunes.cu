@@ -746,14 +746,15 @@ __global__ void __launch_bounds__(kFftThreadsMax) fft_tune_kernel(const FftTuneA
     // the window of the row that starts about one wave of resident blocks
     // later (prefetch.global.L2, one per 128-byte line, addresses within
     // the row).
-    {
+    if (a.stride_s == 1) {  // rows contiguous
         const size_t r2 = rix + a.prefetch_ahead;
         if (r2 < 2 * a.n) {
             const int plane2 = r2 >= a.n ? 1 : 0;
             const size_t i2 = r2 - size_t(plane2) * a.n;
             const size_t bytes = size_t(pl.L) * sizeof(double);
-            const char *rq = reinterpret_cast<const char *>((plane2 ? a.y : a.x) + i2 * a.S + a.from);
-            const char *rp = reinterpret_cast<const char *>((plane2 ? a.py : a.px) + i2 * a.S + a.from);
+            const size_t o2 = i2 * a.stride_i + a.from;
+            const char *rq = reinterpret_cast<const char *>((plane2 ? a.y : a.x) + o2);
+            const char *rp = reinterpret_cast<const char *>((plane2 ? a.py : a.px) + o2);
             const uint32_t lines = uint32_t((bytes + 127u) / 128u) + 1u;
             for (uint32_t l = threadIdx.x; l < 2u * lines; l += blockDim.x) {
                 const size_t off = min(size_t(l % lines) * 128u, bytes - sizeof(double));
@@ -762,7 +763,7 @@ __global__ void __launch_bounds__(kFftThreadsMax) fft_tune_kernel(const FftTuneA
             }
         }
     }
-    if (a.first_nan[i] <= a.last_sample) {  // a NaN sample in the window: NaN tune
+    if (a.first_nan && a.first_nan[i] <= a.last_sample) {  // a NaN sample in the window: NaN tune
         if (threadIdx.x == 0)
             for (int c = 0; c < a.n_out_cols; ++c)
                 a.out[i * a.cols + 2 * size_t(a.out_cols[c]) + plane] = dev::quiet_nan();
@@ -777,12 +778,15 @@ __global__ void __launch_bounds__(kFftThreadsMax) fft_tune_kernel(const FftTuneA
     // order (zeros up to M) for the forward network.  Direct: conj(z_k) at
     // the forward network's position of k, so that the inverse network
     // gives conj(X_k) in natural order (the magnitudes are those of X_k).
+    const size_t o0 = i * a.stride_i + size_t(a.from) * a.stride_s;
+    int nan_seen = 0;
 #pragma unroll 4
     for (uint32_t k = threadIdx.x; k < pl.M; k += blockDim.x) {
         double2 v = make_double2(0.0, 0.0);
         if (k < pl.L) {
-            const size_t o = i * a.S + a.from + k;
+            const size_t o = o0 + size_t(k) * a.stride_s;
             const double re = centred(q[o], a.means, mq), im = centred(p[o], a.means, mp);
+            nan_seen |= isnan(re) || isnan(im);
             const double hk = a.hann[k];
             v = make_double2(re * hk, im * hk);
             if (pl.bluestein) v = c_mul(v, pl.chirp[k]);
@@ -790,7 +794,14 @@ __global__ void __launch_bounds__(kFftThreadsMax) fft_tune_kernel(const FftTuneA
         }
         row[slot<SWZ>(pl.bluestein ? k : pl.pos[k])] = v;
     }
-    __syncthreads();
+    // Without first-NaN records the window's own samples decide
+    // (fft_tune_vec's rule, scanning the window).
+    if (__syncthreads_or(a.first_nan == nullptr && nan_seen)) {
+        if (threadIdx.x == 0)
+            for (int c = 0; c < a.n_out_cols; ++c)
+                a.out[i * a.cols + 2 * size_t(a.out_cols[c]) + plane] = dev::quiet_nan();
+        return;
+    }
     if (pl.bluestein) {
         fft_network<false, SWZ>(row, pl, tc, tf);
         for (uint32_t k = threadIdx.x; k < pl.M; k += blockDim.x)
