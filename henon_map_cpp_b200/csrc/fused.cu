@@ -29,40 +29,53 @@ namespace {
 
 using dev::Rn;
 
-// The windows of one kind that still take samples at sample index idx,
-// as a bit set over the window slots (at most 64 windows per kind; more fall
-// back to testing every window every turn).  Window w is open while
-// idx < limit_w (limit = T + 1 for MEGNO-Birkhoff, the length for
-// Lyapunov, twice the length for the tunes' two windows); `next` is the
-// first index at which an open window closes, when the set is rebuilt.
-// Per turn a warp then visits only its open windows instead of loading
-// and comparing every window's bound.
-struct OpenWindows {
-    uint64_t mask = 0, next = ~0ull;
+// Windows of one kind, sorted by the sample index at which they stop taking
+// samples (every window starts at the construct's first sample, so at any
+// index the open windows are a suffix of this order).  Built per block in
+// shared memory: a turn then walks its open windows with a counter, reading
+// each one's bound and weight pointer as a broadcast, instead of loading
+// bounds and offsets from global memory per window and turn.
+struct WinEntry {
+    const double *w;  // the window's weights
+    uint64_t len;     // MEGNO-Birkhoff: T; Lyapunov: length; tunes: T
+    uint64_t lim;     // first index at which the window is closed
+    double dlen;      // double(len) (Lyapunov's divisor)
+    int orig;         // the window's index in the construct
+    int pad;
 };
 
-template <int KIND>  // 0: MEGNO-Birkhoff (T), 1: Lyapunov (length), 2: tunes (2 length)
-__device__ __forceinline__ uint64_t window_limit(const uint64_t *bound, int w) {
-    const uint64_t b = bound[w];
+template <int KIND>  // 0: MEGNO-Birkhoff (open while idx <= T), 1: Lyapunov
+                     // (idx < length), 2: tunes (two windows, idx < 2 T)
+__device__ __forceinline__ uint64_t window_limit(uint64_t b) {
     return KIND == 0 ? b + 1u : (KIND == 1 ? b : 2u * b);
 }
 
+// Every thread of the block takes part; ties keep the construct's order.
 template <int KIND>
-__device__ __forceinline__ void open_windows(OpenWindows &o, const uint64_t *bound, int n,
-                                             uint64_t idx) {
-    if (n > 64) {  // every window is tested every turn
-        o.next = ~0ull;
-        return;
-    }
-    o.mask = 0;
-    o.next = ~0ull;
-    for (int w = 0; w < n; ++w) {
-        const uint64_t lim = window_limit<KIND>(bound, w);
-        if (idx < lim) {
-            o.mask |= 1ull << w;
-            o.next = lim < o.next ? lim : o.next;
+__device__ __forceinline__ void build_windows(WinEntry *tab, const uint64_t *bound,
+                                              const uint64_t *off, const double *w, int n) {
+    for (int v = int(threadIdx.x); v < n; v += int(blockDim.x)) {
+        const uint64_t lim = window_limit<KIND>(bound[v]);
+        int rank = 0;
+        for (int u = 0; u < n; ++u) {
+            const uint64_t lu = window_limit<KIND>(bound[u]);
+            rank += (lu < lim || (lu == lim && u < v)) ? 1 : 0;
         }
+        WinEntry e;
+        e.w = w + off[v];
+        e.len = bound[v];
+        e.lim = lim;
+        e.dlen = double(bound[v]);
+        e.orig = v;
+        e.pad = 0;
+        tab[rank] = e;
     }
+}
+
+// First open window at index idx, from a previous first open window.
+__device__ __forceinline__ int first_open(const WinEntry *tab, int n, int s, uint64_t idx) {
+    while (s < n && tab[s].lim <= idx) ++s;
+    return s;
 }
 
 // Next sample turn of MEGNO at or after idx (~0 when none).
@@ -109,7 +122,16 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
     double *t1y = t1x + size_t(a.n_tu) * T;
     double *t2x = t1y + size_t(a.n_tu) * T;
     double *t2y = t2x + size_t(a.n_tu) * T;
+    // then the window tables of the three kinds (sorted by closing index);
+    // the accumulators above are kept in table order.
+    WinEntry *tab_mb = reinterpret_cast<WinEntry *>(t2y + size_t(a.n_tu) * T);
+    WinEntry *tab_ly = tab_mb + a.n_mb;
+    WinEntry *tab_tu = tab_ly + a.n_ly;
     const size_t n = a.n;
+    if (DO_M && a.mb_l1) build_windows<0>(tab_mb, a.mb_T, a.mb_off, a.mb_w, a.n_mb);
+    if (DO_V) build_windows<1>(tab_ly, a.ly_len, a.ly_off, a.ly_w, a.n_ly);
+    if (DO_T) build_windows<2>(tab_tu, a.tu_T, a.tu_off, a.tu_w, a.n_tu);
+    __syncthreads();
 
     // ---- load state ---------------------------------------------------------
     double x = a.x[ii], px = a.px[ii], y = a.y[ii], py = a.py[ii];
@@ -127,15 +149,16 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             m_l3 = a.megno_l3[ii];
         }
         if (a.mb_l1) b_l1 = a.mb_l1[ii];
-        for (int w = 0; w < a.n_mb; ++w) mb_l2[w * T + tid] = a.mb_l2[w * n + ii];
+        for (int w = 0; w < a.n_mb; ++w) mb_l2[w * T + tid] = a.mb_l2[tab_mb[w].orig * n + ii];
     }
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (do_v) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) v[k] = a.V[size_t(ii) * 4 + k];
         for (int w = 0; w < a.n_ly; ++w) {
-            ly_raw[w * T + tid] = a.ly_raw[w * n + ii];
-            ly_b[w * T + tid] = a.ly_b[w * n + ii];
+            const size_t g = size_t(tab_ly[w].orig) * n + ii;
+            ly_raw[w * T + tid] = a.ly_raw[g];
+            ly_b[w * T + tid] = a.ly_b[g];
         }
     }
     double store_x = 0.0, store_y = 0.0;
@@ -143,31 +166,23 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
         store_x = a.store_x[ii];
         store_y = a.store_y[ii];
         for (int w = 0; w < a.n_tu; ++w) {
-            t1x[w * T + tid] = a.t1x[w * n + ii];
-            t1y[w * T + tid] = a.t1y[w * n + ii];
-            t2x[w * T + tid] = a.t2x[w * n + ii];
-            t2y[w * T + tid] = a.t2y[w * n + ii];
+            const size_t g = size_t(tab_tu[w].orig) * n + ii;
+            t1x[w * T + tid] = a.t1x[g];
+            t1y[w * T + tid] = a.t1y[g];
+            t2x[w * T + tid] = a.t2x[g];
+            t2y[w * T + tid] = a.t2y[g];
         }
     }
 
     const double mu = a.mu;
     const dev::Barrier bar = dev::make_barrier<HM_ARITH_EXACT>(a.b2bits);
     bool warp_live = __any_sync(dev::kFullMask, alive);
-    // Two open-window sets per thread (registers): a thread with the matrix
-    // work keeps its MEGNO-Birkhoff windows in the first and its next MEGNO
-    // sample turn in the second's `next`; a thread with the vector or tune
-    // work its Lyapunov windows in the first and its tune windows in the
-    // second.  No thread has both (the matrix work is split from the others
-    // whenever both are asked for), and a kind left without a set tests
-    // every window every turn.
-    const bool snap_in_b = do_m && a.megno_l1 && a.n_snap > 0;
-    const bool all_mb = a.n_mb > 64, all_ly = a.n_ly > 64 || (do_m && a.mb_l1),
-               all_tu = a.n_tu > 64 || snap_in_b;
-    OpenWindows setA, setB;
-    if (do_m && a.mb_l1 && !all_mb) open_windows<0>(setA, a.mb_T, a.n_mb, a.mb_idx);
-    else if (do_v && a.n_ly && !all_ly) open_windows<1>(setA, a.ly_len, a.n_ly, a.ly_idx);
-    if (snap_in_b) setB.next = next_sample(a.snap_turns, a.n_snap, a.megno_idx);
-    else if (do_t && !all_tu) open_windows<2>(setB, a.tu_T, a.n_tu, a.tu_idx);
+    // First open window of each kind, and the next MEGNO sample turn.
+    const bool snaps = do_m && a.megno_l1 && a.n_snap > 0;
+    uint64_t next_snap = snaps ? next_sample(a.snap_turns, a.n_snap, a.megno_idx) : ~0ull;
+    int s_mb = first_open(tab_mb, a.mb_l1 ? a.n_mb : 0, 0, a.mb_idx);
+    int s_ly = first_open(tab_ly, a.n_ly, 0, a.ly_idx);
+    int s_tu = first_open(tab_tu, a.n_tu, 0, a.tu_idx);
     uint32_t k = 0;
     for (; k < a.n_turns && warp_live; ++k) {
         double df[16];
@@ -233,30 +248,20 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
                 m_l2 = Rn::add(m_l2, Rn::mul(inv, m_l1));
                 m_l3 = Rn::mul(inv, m_l2);
                 const uint64_t cur = a.megno_idx + k;
-                if (snap_in_b && cur == setB.next) {  // a sample turn: every slot that asks
+                if (cur == next_snap) {  // a sample turn: every slot that asks
                     for (int j = 0; j < a.n_snap; ++j)
                         if (a.snap_turns[j] == cur && in_range) a.snap[size_t(j) * n + ii] = m_l3;
-                    setB.next = next_sample(a.snap_turns, a.n_snap, cur + 1u);
+                    next_snap = next_sample(a.snap_turns, a.n_snap, cur + 1u);
                 }
             }
             if (a.mb_l1) {
                 const uint64_t idx = a.mb_idx + k;
                 const double di = double(idx);
                 b_l1 = Rn::add(b_l1, Rn::mul(lr, di));
-                if (all_mb) {
-                    for (int w = 0; w < a.n_mb; ++w)
-                        if (idx <= a.mb_T[w]) {
-                            double &acc = mb_l2[w * T + tid];
-                            acc = Rn::add(acc,
-                                          Rn::div(Rn::mul(b_l1, a.mb_w[a.mb_off[w] + idx - 1]), di));
-                        }
-                } else {
-                    if (idx >= setA.next) open_windows<0>(setA, a.mb_T, a.n_mb, idx);
-                    for (uint64_t m = setA.mask; m; m &= m - 1u) {
-                        const int w = __ffsll(static_cast<long long>(m)) - 1;
-                        double &acc = mb_l2[w * T + tid];
-                        acc = Rn::add(acc, Rn::div(Rn::mul(b_l1, a.mb_w[a.mb_off[w] + idx - 1]), di));
-                    }
+                s_mb = first_open(tab_mb, a.n_mb, s_mb, idx);
+                for (int w = s_mb; w < a.n_mb; ++w) {
+                    double &acc = mb_l2[w * T + tid];
+                    acc = Rn::add(acc, Rn::div(Rn::mul(b_l1, tab_mb[w].w[idx - 1]), di));
                 }
             }
             old_norm = new_norm;
@@ -279,20 +284,11 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             if (a.n_ly) {
                 const double l = log(nv);
                 const uint64_t idx = a.ly_idx + k;
-                if (!all_ly && idx >= setA.next) open_windows<1>(setA, a.ly_len, a.n_ly, idx);
-                uint64_t m = all_ly ? 0u : setA.mask;
-                for (int w = all_ly ? 0 : -1; all_ly ? w < a.n_ly : m != 0u;) {
-                    if (!all_ly) {
-                        w = __ffsll(static_cast<long long>(m)) - 1;
-                        m &= m - 1u;
-                    }
-                    const uint64_t len = a.ly_len[w];
-                    if (idx < len) {
-                        ly_raw[w * T + tid] = Rn::add(ly_raw[w * T + tid], Rn::div(l, double(len)));
-                        ly_b[w * T + tid] =
-                            Rn::add(ly_b[w * T + tid], Rn::mul(l, a.ly_w[a.ly_off[w] + idx]));
-                    }
-                    if (all_ly) ++w;
+                s_ly = first_open(tab_ly, a.n_ly, s_ly, idx);
+                for (int w = s_ly; w < a.n_ly; ++w) {
+                    const WinEntry &e = tab_ly[w];
+                    ly_raw[w * T + tid] = Rn::add(ly_raw[w * T + tid], Rn::div(l, e.dlen));
+                    ly_b[w * T + tid] = Rn::add(ly_b[w * T + tid], Rn::mul(l, e.w[idx]));
                 }
             }
 #pragma unroll
@@ -307,20 +303,15 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             store_x = ax;
             store_y = ay;
             const uint64_t idx = a.tu_idx + k;
-            if (!all_tu && idx >= setB.next) open_windows<2>(setB, a.tu_T, a.n_tu, idx);
-            uint64_t m = all_tu ? 0u : setB.mask;
-            for (int w = all_tu ? 0 : -1; all_tu ? w < a.n_tu : m != 0u; w = all_tu ? w + 1 : w) {
-                if (!all_tu) {
-                    w = __ffsll(static_cast<long long>(m)) - 1;
-                    m &= m - 1u;
-                }
-                const uint64_t len = a.tu_T[w];
-                if (idx < len) {
-                    const double wt = a.tu_w[a.tu_off[w] + idx];
+            s_tu = first_open(tab_tu, a.n_tu, s_tu, idx);
+            for (int w = s_tu; w < a.n_tu; ++w) {
+                const WinEntry &e = tab_tu[w];
+                if (idx < e.len) {  // first window [0, T)
+                    const double wt = e.w[idx];
                     t1x[w * T + tid] = Rn::add(t1x[w * T + tid], Rn::mul(dx, wt));
                     t1y[w * T + tid] = Rn::add(t1y[w * T + tid], Rn::mul(dy, wt));
-                } else if (idx < 2 * len) {
-                    const double wt = a.tu_w[a.tu_off[w] + idx - len];
+                } else {  // second window [T, 2 T)
+                    const double wt = e.w[idx - e.len];
                     t2x[w * T + tid] = Rn::add(t2x[w * T + tid], Rn::mul(dx, wt));
                     t2y[w * T + tid] = Rn::add(t2y[w * T + tid], Rn::mul(dy, wt));
                 }
@@ -344,12 +335,12 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
         if (do_m && a.mb_l1) {
             const uint64_t idx = a.mb_idx + k;
             for (int w = 0; w < a.n_mb; ++w)
-                if (idx <= a.mb_T[w]) mb_l2[w * T + tid] = nan;
+                if (idx <= tab_mb[w].len) mb_l2[w * T + tid] = nan;
         }
         if (do_v) {
             const uint64_t idx = a.ly_idx + k;
             for (int w = 0; w < a.n_ly; ++w)
-                if (idx < a.ly_len[w]) {
+                if (idx < tab_ly[w].len) {
                     ly_raw[w * T + tid] = nan;
                     ly_b[w * T + tid] = nan;
                 }
@@ -357,7 +348,7 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
         if (do_t) {
             const uint64_t first = a.tu_idx + k, last = a.tu_idx + k + left - 1;
             for (int w = 0; w < a.n_tu; ++w) {
-                const uint64_t len = a.tu_T[w];
+                const uint64_t len = tab_tu[w].len;
                 if (first < len) {
                     t1x[w * T + tid] = nan;
                     t1y[w * T + tid] = nan;
@@ -389,24 +380,26 @@ __global__ void __launch_bounds__(128, SPLIT ? 4 : 1) indicators_kernel(const Fu
             a.megno_l3[i] = m_l3;
         }
         if (a.mb_l1) a.mb_l1[i] = b_l1;
-        for (int w = 0; w < a.n_mb; ++w) a.mb_l2[w * n + i] = mb_l2[w * T + tid];
+        for (int w = 0; w < a.n_mb; ++w) a.mb_l2[tab_mb[w].orig * n + i] = mb_l2[w * T + tid];
     }
     if (do_v) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) a.V[size_t(i) * 4 + q] = v[q];
         for (int w = 0; w < a.n_ly; ++w) {
-            a.ly_raw[w * n + i] = ly_raw[w * T + tid];
-            a.ly_b[w * n + i] = ly_b[w * T + tid];
+            const size_t g = size_t(tab_ly[w].orig) * n + i;
+            a.ly_raw[g] = ly_raw[w * T + tid];
+            a.ly_b[g] = ly_b[w * T + tid];
         }
     }
     if (do_t) {
         a.store_x[i] = store_x;
         a.store_y[i] = store_y;
         for (int w = 0; w < a.n_tu; ++w) {
-            a.t1x[w * n + i] = t1x[w * T + tid];
-            a.t1y[w * n + i] = t1y[w * T + tid];
-            a.t2x[w * n + i] = t2x[w * T + tid];
-            a.t2y[w * n + i] = t2y[w * T + tid];
+            const size_t g = size_t(tab_tu[w].orig) * n + i;
+            a.t1x[g] = t1x[w * T + tid];
+            a.t1y[g] = t1y[w * T + tid];
+            a.t2x[g] = t2x[w * T + tid];
+            a.t2y[g] = t2y[w * T + tid];
         }
     }
 }
@@ -419,7 +412,8 @@ cudaError_t launch4(const FusedArgs &a, cudaStream_t s) {
     constexpr bool split = DO_M && (DO_V || DO_T);
     constexpr int per_block = split ? threads / 2 : threads;  // particles
     const size_t slots = size_t(a.n_mb) + 2 * size_t(a.n_ly) + 4 * size_t(a.n_tu);
-    const size_t smem = slots * per_block * sizeof(double);
+    const size_t tables = (size_t(a.n_mb) + a.n_ly + a.n_tu) * sizeof(WinEntry);
+    const size_t smem = slots * per_block * sizeof(double) + tables;
     auto k = indicators_kernel<OCT, DO_M, DO_V, DO_T, split>;
     if (smem > 48 * 1024) {
         const cudaError_t e =
