@@ -516,10 +516,13 @@ __global__ void fft_peak_kernel(const double2 *buf, uint32_t len, size_t count,
 // which takes natural order in and leaves X_k at a digit-reversed position
 // (FftPlanDev::pos).  The inverse network runs the stages backwards with
 // conjugate twiddles applied before each butterfly (decimation in time),
-// which takes that order back to natural order (times M).  Bluestein's
-// convolution (L. Bluestein, "A linear filtering approach to the
+// which takes that order back to natural order (times M).  A window whose
+// length has no prime factor above 5 is transformed directly (M = L): its
+// samples, conjugated, are loaded at the forward network's positions, and
+// the inverse network returns conj(X_k) in natural order.  Other lengths
+// take Bluestein's convolution (L. Bluestein, "A linear filtering approach to the
 // computation of the discrete Fourier transform", IEEE Trans. Audio
-// Electroacoust. 18 (1970) 451-455) uses both:
+// Electroacoust. 18 (1970) 451-455), which uses both networks:
 //     X_k = c_k sum_n (z_n c_n) conj(c_{k-n}),  c_n = exp(-i pi n^2 / L),
 // the cyclic convolution of length M >= 2L - 1 being the inverse network of
 // the pointwise product of the forward network's outputs (that of b_m =
