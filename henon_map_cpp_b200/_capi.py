@@ -181,6 +181,8 @@ _SIGNATURES = {
     "hm_tracker_orbit_tunes": (None, [c_void_p, c_void_p, c_uint32, c_double, c_double,
                                       c_double, c_int, _PU32, _PU32, c_size_t, c_int, _PD, _PD]),
     "hm_storage_tunes": (None, [c_void_p, _PU32, _PU32, c_size_t, c_int, _PD]),
+    "hm_set_tune_slice_limit": (None, [c_size_t]),
+    "hm_get_tune_slice_limit": (None, [POINTER(c_size_t)]),
     "hm_orbit_tunes_host": (None, [_PD, _PD, _PD, _PD, c_size_t, c_size_t, _PU32, _PU32,
                                    c_size_t, c_int, _PD]),
     # orbit-loss gradients

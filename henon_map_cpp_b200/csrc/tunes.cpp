@@ -2,6 +2,7 @@
 // hm_storage_tunes): window validation, Birkhoff weight tables, cuFFT
 // plans, and particle slicing so orbit buffers fit device memory.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -212,6 +213,9 @@ namespace {
 // running it at these sizes.  Plans hold no work area of their own: each
 // call lends one from the library's pool (released with the call), so a
 // cached plan keeps no device memory between calls.
+// Process-wide cap on the particles of one tune slice (0: none).
+std::atomic<size_t> g_tune_slice_limit{0};
+
 struct CachedPlan {
     cufftHandle plan = 0;
     size_t work = 0;  // bytes of work area an execution needs
@@ -395,7 +399,8 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
                                 (max_len ? 2 * (size_t(max_len) * sizeof(double2) +
                                                 fft_work_per_row(max_len))
                                          : 0u);
-    const size_t slice = std::max<size_t>(1, std::min<size_t>(n, (free_b / 3 * 2) / per_particle));
+    size_t slice = std::max<size_t>(1, std::min<size_t>(n, (free_b / 3 * 2) / per_particle));
+    if (const size_t cap = g_tune_slice_limit.load(); cap > 0) slice = std::min(slice, cap);
     const size_t m0 = std::min(n, slice);
     // Segments of the Birkhoff sums: enough threads to fill the device.
     const uint32_t seg_len = std::max<uint32_t>(64u, uint32_t(std::min<size_t>(
@@ -509,6 +514,17 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
         p->global_steps += n_turns;
         p->live_step += n_turns;
     }
+    return ok();
+}
+
+hm_status hm_set_tune_slice_limit(size_t max_particles) {
+    g_tune_slice_limit.store(max_particles);
+    return ok();
+}
+
+hm_status hm_get_tune_slice_limit(size_t *max_particles) {
+    if (!max_particles) return fail(HM_ERR_INVALID_ARG, "null output");
+    *max_particles = g_tune_slice_limit.load();
     return ok();
 }
 

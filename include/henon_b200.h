@@ -504,6 +504,13 @@ hm_status hm_tracker_orbit_tunes(hm_tracker *t, hm_particles *p, uint32_t n_turn
                                  const uint32_t *to, size_t n_windows,
                                  int remove_mean, double *birkhoff_out,
                                  double *fft_out);
+/* Most particles hm_tracker_orbit_tunes records in one slice (0, the
+ * default: as many as two thirds of the free device memory hold).  A cap
+ * bounds the call's device memory; the FFT tunes and the orbit do not
+ * depend on it, the Birkhoff sums only through their segments (1e-13).
+ * Process-wide. */
+hm_status hm_set_tune_slice_limit(size_t max_particles);
+hm_status hm_get_tune_slice_limit(size_t *max_particles);
 /* Tunes of a storage's snapshots (storage_4d::tune_birkhoff / tune_fft,
  * src/henon.cu:3261-3329). */
 hm_status hm_storage_tunes(const hm_storage *s, const uint32_t *from,

@@ -3,6 +3,8 @@ tracker's whole-orbit tunes and MEGNO, storage tunes) against the oracle
 (oracle/tunes.py) and the values recorded in the reference's notebooks."""
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -87,6 +89,37 @@ def test_tracker_fft_tunes_window_lengths(gpu, remove_mean):
                      for i in range(x.size)])
     assert np.isfinite(want).all()
     _close(f, want, 1e-10, "fft")
+
+
+def test_tracker_orbit_tunes_in_slices(gpu):
+    # A cap on the particles of one slice (hm_set_tune_slice_limit) splits
+    # the orbit into slices of 7 particles: every slice's record continues the
+    # same particles (kicks keyed by the global index), the FFT rows are the
+    # same rows, and only the Birkhoff sums' segments change (1e-13).
+    x, px, y, py = grid(0.3, 5, px0=0.001)
+    frm, to = [0, 100, 300], [99, 700, 1500]
+
+    def run(limit):
+        C.call("hm_set_tune_slice_limit", limit)
+        try:
+            tr = C.Tracker(1500, *TUNES, "sps", NAN, 16.0, 0)
+            p = C.Particles(x, px, y, py)
+            p.kick_seed = 77
+            b, f = C.tracker_orbit_tunes(tr, p, 1500, 0.2, 10.0, frm, to, True, True,
+                                         kick_module=1e-7)
+            return b, f, p.get(C.FIELD_X), p.get(C.FIELD_STEPS)
+        finally:
+            C.call("hm_set_tune_slice_limit", 0)
+
+    b0, f0, x0, s0 = run(0)
+    b7, f7, x7, s7 = run(7)
+    assert_bitwise(f7, f0)
+    assert_bitwise(x7, x0)
+    np.testing.assert_array_equal(s7, s0)
+    _close(b7, b0, 1e-13, "birkhoff")
+    got = ctypes.c_size_t(1)
+    C.call("hm_get_tune_slice_limit", ctypes.byref(got))
+    assert got.value == 0
 
 
 def test_storage_tunes_match_oracle(gpu):
