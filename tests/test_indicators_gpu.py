@@ -282,27 +282,48 @@ def test_storage_and_matrix_helpers(gpu):
         C.TuneBirkhoff(n, [5]).add(p)
 
 
-def test_fused_many_windows_take_the_every_window_path(gpu):
-    # More than 64 windows of one kind (here 70 MEGNO-Birkhoff windows) are
-    # tested every turn instead of through the open-window bit set; both
-    # must give the per-call loop's values.
+def test_fused_many_windows_in_any_order(gpu):
+    # The fused kernel sorts each kind's windows by closing index into a
+    # table and keeps the accumulators in that order: 40 MEGNO-Birkhoff
+    # windows and 8 Lyapunov and 8 tune windows (88 of the 96 accumulator
+    # slots), given out of order and with repeated lengths, must come back
+    # in the construct's order with the per-call loop's values.
+    rng = np.random.default_rng(11)
     x, px, y, py = grid(0.5, 6)
     n, n_turns = x.size, 300
-    mb_w = [int(t) for t in np.linspace(5, 400, 70).round()]
+    mb_w = [int(t) for t in rng.permutation(np.r_[np.linspace(5, 400, 37).round(), 5, 100, 300])]
+    ly_w = [int(t) for t in rng.permutation([3, 50, 50, 120, 299, 300, 301, 1])]
+    tu_w = [int(t) for t in rng.permutation([2, 40, 40, 150, 151, 75, 149, 10])]
     t = C.Tracker(n_turns + 1, TUNES[0], TUNES[1], "sps", NAN, 16.0, 0)
     p = C.Particles(x, px, y, py)
     M, Mo, mg, mb = C.Matrices(n), C.Matrices(n), C.Megno(n), C.MegnoBirkhoff(n, mb_w)
+    V, ly, tu = C.Vectors(np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))), C.Lyapunov(n, ly_w), C.TuneBirkhoff(n, tu_w)
+    tu.first_add(p)
     C.track_indicators(t, p, n_turns, 0.2, 10.0, matrix=M, matrix_old=Mo, megno=mg,
-                       megno_birkhoff=mb, megno_sample_turns=[7, 300], megno_samples_out=None)
+                       megno_birkhoff=mb, vectors=V, lyapunov=ly, tune=tu,
+                       megno_sample_turns=[7, 300], megno_samples_out=None)
     t2 = C.Tracker(n_turns + 1, TUNES[0], TUNES[1], "sps", NAN, 16.0, 0)
     p2 = C.Particles(x, px, y, py)
     M2, Mo2, mg2, mb2 = C.Matrices(n), C.Matrices(n), C.Megno(n), C.MegnoBirkhoff(n, mb_w)
+    V2, ly2, tu2 = C.Vectors(np.tile([1.0, 0.0, 0.0, 0.0], (n, 1))), C.Lyapunov(n, ly_w), C.TuneBirkhoff(n, tu_w)
+    tu2.first_add(p2)
+    J = C.Matrices(n)
     for _ in range(n_turns):
         Mo2.explicit_copy(M2)
         t2.track(p2, 1, 0.2, 10.0)
         M2.structured_multiply(t2, p2, 0.2)
         mg2.add(M2, Mo2)
         mb2.add(M2, Mo2)
-    assert_bitwise(mb.get(), mb2.get(), "megno birkhoff, 70 windows")
+        J.set_with_tracker(t2, p2, 0.2)
+        V2.multiply(J)
+        ly2.add(V2)
+        V2.normalize()
+        tu2.add(p2)
+    assert_bitwise(mb.get(), mb2.get(), "megno birkhoff, 40 windows")
     assert_bitwise(mg.get(), mg2.get(), "megno")
     assert_bitwise(M.get(), M2.get(), "matrices")
+    assert_bitwise(V.get(), V2.get(), "vectors")
+    assert_bitwise(ly.get(False), ly2.get(False), "lyapunov")
+    assert_bitwise(ly.get(True), ly2.get(True), "lyapunov birkhoff")
+    for j in range(4):
+        assert_bitwise(tu.get(j), tu2.get(j), f"tunes {j}")
