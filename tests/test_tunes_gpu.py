@@ -91,6 +91,29 @@ def test_tracker_fft_tunes_window_lengths(gpu, remove_mean):
     _close(f, want, 1e-10, "fft")
 
 
+@pytest.mark.parametrize("remove_mean", [False, True])
+def test_fft_tunes_of_a_resting_particle(gpu, remove_mean):
+    # A particle at the origin stays there: every window's spectrum is zero,
+    # whose first maximum is bin 0, so the FFT tune is 1.0 on the direct
+    # (1000, 2^3 5^3), Bluestein (1001, 4001) and library (12801) transforms
+    # alike, as in the oracle; the moving particle beside it is compared too.
+    x = np.array([0.0, 0.1])
+    z = np.zeros(2)
+    y = np.array([0.0, 0.1])
+    n_turns = 13000
+    frm, to = [0, 10, 100, 0], [999, 1010, 4100, 12800]
+    tr = C.Tracker(n_turns, *TUNES, "sps", NAN, 0.0, 0)
+    p = C.Particles(x, z, y, z)
+    b, f = C.tracker_orbit_tunes(tr, p, n_turns, 0.0, 10.0, frm, to, remove_mean, True)
+    assert (f[0] == 1.0).all()
+    orb = T.orbit(x, z, y, z, O.tables(n_turns, *TUNES, "sps", epsilon=0.0), n_turns, 0.0)
+    if remove_mean:
+        orb = T.remove_mean(orb)
+    want = np.array([T.tune_vec(*(orb[c, :, i] for c in range(4)), frm, to, "fft")
+                     for i in range(2)])
+    _close(f, want, 1e-10, "fft")
+
+
 def test_tracker_orbit_tunes_in_slices(gpu):
     # A cap on the particles of one slice (hm_set_tune_slice_limit) splits
     # the orbit into slices of 7 particles: every slice's record continues the
