@@ -217,14 +217,18 @@ t = cls_t(int(d["n_turns"]), float(d["tunes"][0]), float(d["tunes"][1]), "sps", 
           float(d["epsilon"]), 0)
 p = cls_p(d["x"], d["px"], d["y"], d["py"])
 t.track(p, int(d["n_turns"]), float(d["mu"]), float(d["barrier"]))
+if int(d["n_back"]):
+    t.track(p, int(d["n_back"]), float(d["mu"]), float(d["barrier"]), float("nan"), True)
 np.savez(sys.argv[4], x=np.asarray(p.get_x()), px=np.asarray(p.get_px()),
          y=np.asarray(p.get_y()), py=np.asarray(p.get_py()), steps=np.asarray(p.get_steps()))
 """
 
 
 def reference_track_subprocess(variant: str, x, px, y, py, n_turns: int, tunes, epsilon: float,
-                               mu: float, barrier: float = 10.0, gpu: bool = True):
-    """Tracks with the reference build `variant` in a child interpreter.
+                               mu: float, barrier: float = 10.0, gpu: bool = True,
+                               n_back: int = 0):
+    """Tracks with the reference build `variant` in a child interpreter:
+    n_turns forward, then n_back backward (track(..., inverse=True)).
 
     Two builds of the reference share one pybind11 module name, so only one
     of them can live in a process; the child keeps them apart.  Returns
@@ -237,7 +241,7 @@ def reference_track_subprocess(variant: str, x, px, y, py, n_turns: int, tunes, 
         inp, out = Path(tmp) / "in.npz", Path(tmp) / "out.npz"
         np.savez(inp, x=np.asarray(x, float), px=np.asarray(px, float), y=np.asarray(y, float),
                  py=np.asarray(py, float), n_turns=n_turns, tunes=np.asarray(tunes, float),
-                 epsilon=epsilon, mu=mu, barrier=barrier, gpu=int(gpu))
+                 epsilon=epsilon, mu=mu, barrier=barrier, gpu=int(gpu), n_back=int(n_back))
         subprocess.run([sys.executable, "-c", _CHILD, str(HERE.parent), variant, str(inp),
                         str(out)], check=True)
         d = np.load(out)

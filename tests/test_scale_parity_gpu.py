@@ -16,6 +16,9 @@ own CUDA path built with --fmad=false (oracle/_ref/fmad_off).
   (src/henon.cu:1694-2655) bit for bit.
 * The inverse tangent matrix (inverse_tangent_matrix, src/henon.cu:224-249)
   through get_tangent_matrix(..., reverse=True).
+* Backward tracking (track(..., inverse=True): the reverse turn with
+  table[steps - 1], steps decreasing, src/henon.cu:510-528) after forward
+  turns, on a 256^2 grid, against the reference's GPU tracker.
 """
 from __future__ import annotations
 
@@ -165,3 +168,27 @@ def test_reverse_tangent_matrix_vs_reference_gpu(gpu, mu):
         theirs = np.asarray(rt.get_tangent_matrix(rp, mu, reverse), dtype=np.float64)
         assert_bitwise(ours.reshape(theirs.shape), theirs, f"reverse={reverse}")
         assert np.isfinite(ours).any()
+
+
+@needs_ref
+@pytest.mark.parametrize("mu", [0.0, 0.2])
+def test_backward_tracking_bit_exact_vs_reference_gpu(gpu, mu):
+    v = np.linspace(0.0, 0.5, 256)
+    xx, yy = np.meshgrid(v, v)
+    x, y = xx.ravel(), yy.ravel()
+    px = np.full_like(x, 1e-3)
+    py = np.zeros_like(x)
+    n_fwd, n_back = 3000, 2000
+    ref = O.reference_track_subprocess("fmad_off", x, px, y, py, n_fwd, TUNES, 16.0, mu, 10.0,
+                                       gpu=True, n_back=n_back)
+    t = C.Tracker(n_fwd, TUNES[0], TUNES[1], "sps", NAN, 16.0, 0)
+    p = C.Particles(x, px, y, py)
+    t.track(p, n_fwd, mu, 10.0)
+    t.track(p, n_back, mu, 10.0, float("nan"), True)
+    got = p.state()
+    np.testing.assert_array_equal(got[4], ref[4], err_msg=f"steps mu={mu}")
+    for a, b, name in zip(got[:4], ref[:4], ("x", "px", "y", "py")):
+        assert_bitwise(a, b, f"{name} mu={mu}")
+    assert p.global_steps == n_fwd - n_back
+    lost = np.isnan(got[0])
+    assert lost.any() and not lost.all()
