@@ -16,6 +16,8 @@ own CUDA path built with --fmad=false (oracle/_ref/fmad_off).
   (src/henon.cu:1694-2655) bit for bit.
 * The inverse tangent matrix (inverse_tangent_matrix, src/henon.cu:224-249)
   through get_tangent_matrix(..., reverse=True).
+* The scan's second horizon, 10^6 turns, on every 16th point of the
+  1024^2 grid per axis (4096 particles) for two of the six scans.
 * Backward tracking (track(..., inverse=True): the reverse turn with
   table[steps - 1], steps decreasing, src/henon.cu:510-528) after forward
   turns, on a 256^2 grid, against the reference's GPU tracker.
@@ -192,3 +194,21 @@ def test_backward_tracking_bit_exact_vs_reference_gpu(gpu, mu):
     assert p.global_steps == n_fwd - n_back
     lost = np.isnan(got[0])
     assert lost.any() and not lost.all()
+
+
+@needs_ref
+@pytest.mark.parametrize("eps,mu", [(1.0, 0.0), (64.0, 0.2)])
+def test_long_horizon_subsample_bit_exact_vs_reference_gpu(gpu, eps, mu):
+    x, px, y, py = (c.reshape(SCAN_SIDE, SCAN_SIDE)[::16, ::16].ravel() for c in _scan_grid())
+    n_turns = 1_000_000
+    ref = O.reference_track_subprocess("fmad_off", x, px, y, py, n_turns, TUNES, eps, mu, 10.0,
+                                       gpu=True)
+    t = C.Tracker(n_turns, TUNES[0], TUNES[1], "sps", NAN, eps, 0)
+    p = C.Particles(x, px, y, py)
+    t.track(p, n_turns, mu, 10.0)
+    got = p.state()
+    np.testing.assert_array_equal(got[4], ref[4], err_msg=f"steps eps={eps} mu={mu}")
+    for a, b, name in zip(got[:4], ref[:4], ("x", "px", "y", "py")):
+        assert_bitwise(a, b, f"{name} eps={eps} mu={mu}")
+    survivors = int(np.sum(got[4] == n_turns))
+    assert 0 < survivors < x.size
