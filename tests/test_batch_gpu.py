@@ -177,3 +177,27 @@ def test_job_list_runs_as_one_batch_like_run_sim(gpu, tmp_path):
                 np.testing.assert_array_equal(f["steps"][...], want)
         else:
             np.testing.assert_array_equal(np.load(npz)["steps"], want)
+
+
+def test_batch_sets_equal_reference_gpu_tracker(gpu):
+    # Each set of a batch against the reference's own GPU tracker built with
+    # --fmad=false (henon_tracker_gpu::track, src/henon.cu:3155-3185), set by
+    # set: coordinates bit for bit and survival turns.
+    from oracle import oracle as O
+
+    if not (O.REF_DIR / "fmad_off").exists():
+        pytest.skip("reference build absent")
+    sets, coords = sweep.heterogeneous_sets(seed=23, n_sets=5, n_range=(300, 5000),
+                                            turn_range=(500, 20000))
+    res = sweep.run_sweep(sets, coords, arith=C.ARITH_EXACT)
+    o = 0
+    for s, r in zip(sets, res):
+        n = s["n_particles"]
+        part = [c[o:o + n] for c in coords]
+        o += n
+        want = O.reference_track_subprocess("fmad_off", *part, s["n_turns"],
+                                            (s["omega_x"], s["omega_y"]), s["epsilon"], s["mu"],
+                                            s["barrier"], gpu=True)
+        np.testing.assert_array_equal(r["steps"], want[4])
+        for k, w in zip(("x", "px", "y", "py"), want[:4]):
+            assert_bitwise(r[k], w, k)
